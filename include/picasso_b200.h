@@ -1,0 +1,297 @@
+/*
+ * picasso_b200.h -- C ABI of the B200 particle/grid transfer library.
+ *
+ * The library re-implements the particle-to-grid (P2G) and grid-to-particle
+ * (G2P) transfers of Picasso (APIC and PolyPIC) on the uniform Cartesian mesh,
+ * the B-spline stencil evaluation they use, the particle cell-sort that feeds
+ * the tiled kernels, the grid velocity update between P2G and G2P, and the
+ * batched 3x3 linear algebra used by PolyPIC.
+ *
+ * Every entry point takes plain pointers, sizes and POD descriptors; device
+ * pointers are CUDA device memory on the current device.  All launches are
+ * asynchronous on the stream in picasso_exec; a returned PICASSO_OK means the
+ * arguments were valid and the work was enqueued.  No exceptions cross the ABI.
+ *
+ * Reference interfaces replaced (paths inside the Picasso source tree):
+ *   Picasso::APIC::p2g / g2p          src/Picasso_APIC.hpp:55-544
+ *   Picasso::PolyPIC::p2g / g2p       src/Picasso_PolyPIC.hpp:39-359
+ *   Picasso::createSpline             src/Picasso_ParticleInterpolation.hpp:88-105
+ *   GridOperator::apply over particles (particle loop + ScatterView zero /
+ *     contribute)                     src/Picasso_GridOperator.hpp:403-429,521-591,612-642
+ *   LinearAlgebra::operator! / inverse (3x3)
+ *                                     src/Picasso_BatchedLinearAlgebra.hpp:4337-4350,4626-4686
+ */
+#ifndef PICASSO_B200_H
+#define PICASSO_B200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define PICASSO_API __attribute__((visibility("default")))
+#else
+#define PICASSO_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Status codes                                                             */
+/* ------------------------------------------------------------------------ */
+typedef enum picasso_status {
+    PICASSO_OK = 0,
+    PICASSO_ERR_INVALID_ARGUMENT = 1, /* bad descriptor, size, dtype combination */
+    PICASSO_ERR_UNSUPPORTED = 2,      /* valid but not implemented combination */
+    PICASSO_ERR_CUDA = 3,             /* a CUDA runtime call failed */
+    PICASSO_ERR_OUT_OF_RANGE = 4,     /* key / index range exceeds the format */
+    PICASSO_ERR_TIMEOUT = 5,          /* a bounded device wait gave up */
+    PICASSO_ERR_NO_DEVICE = 6         /* no usable sm_100 device */
+} picasso_status;
+
+/* Element types of particle and grid arrays. */
+typedef enum picasso_dtype {
+    PICASSO_F64 = 0,
+    PICASSO_F32 = 1,
+    PICASSO_I64_FIXED = 2 /* signed 64-bit fixed point: value = raw * 2^-fixed_bits */
+} picasso_dtype;
+
+/* Mesh entity the spline is defined on (Picasso FieldLocation / Cabana::Grid
+ * entity types).  Face<D>: on nodes along D, on cell centres along the other
+ * two dimensions.  Edge<D>: on cell centres along D, on nodes elsewhere. */
+typedef enum picasso_location {
+    PICASSO_NODE = 0,
+    PICASSO_CELL = 1,
+    PICASSO_FACE_I = 2,
+    PICASSO_FACE_J = 3,
+    PICASSO_FACE_K = 4,
+    PICASSO_EDGE_I = 5,
+    PICASSO_EDGE_J = 6,
+    PICASSO_EDGE_K = 7
+} picasso_location;
+
+/* ------------------------------------------------------------------------ */
+/* Descriptors                                                              */
+/* ------------------------------------------------------------------------ */
+
+/* Local uniform mesh.  Index space of the grid arrays passed to a call: entity
+ * (i,j,k) with 0 <= i < extent[0] etc. (ghost layers included, as in a
+ * Cabana::Grid local array).  Physical coordinate of entity (i,j,k) along d:
+ *     low_corner[d] + (index[d] + offset_d(location)) * cell_size[d]
+ * with offset 0 (node-aligned) or 0.5 (cell-centre-aligned).
+ * periodic[d] != 0: stencil indices are wrapped into
+ *     [own_begin[d], own_begin[d] + own_extent[d])
+ * so that all periodic images accumulate into the owned entity (what the
+ * reference's halo Sum scatter does after P2G and its halo gather provides
+ * before G2P).  Non-periodic: a particle whose stencil leaves
+ * [0, extent[d]) is skipped and counted in picasso_exec.error_count. */
+typedef struct picasso_mesh {
+    int32_t extent[3];
+    int32_t own_begin[3];
+    int32_t own_extent[3];
+    int32_t periodic[3];
+    double low_corner[3];
+    double cell_size[3];
+} picasso_mesh;
+
+/* Equivalent of createSpline(Location, InterpolationOrder<order>, mesh, x):
+ * the spline is evaluated inside the kernels from each particle position. */
+typedef struct picasso_spline {
+    picasso_mesh mesh;
+    int32_t location; /* picasso_location */
+    int32_t order;    /* 1 (linear), 2 (quadratic), 3 (cubic) */
+} picasso_spline;
+
+/* Particle member.  Element (p, c) of a member with C components lives at
+ *   data + ((p >> vector_shift) * tile_stride + c * comp_stride
+ *           + (p & ((1 << vector_shift) - 1)))        [in elements]
+ * which covers plain structure-of-arrays (vector_shift >= 62, comp_stride =
+ * number of particles), array-of-structures (vector_shift = 0, tile_stride =
+ * C, comp_stride = 1) and Cabana AoSoA storage (vector_shift = log2 of the
+ * vector length, tile_stride = elements per SoA, comp_stride = vector length,
+ * data = the member's first element).  Matrix members c_p(r, d) use component
+ * index c = r * ncomp + d, which is Cabana's row-major matrix member layout. */
+typedef struct picasso_particle_field {
+    void* data;
+    int32_t dtype;        /* picasso_dtype (F64 or F32) */
+    int32_t vector_shift; /* log2 of the AoSoA vector length; >= 62 for SoA */
+    int64_t tile_stride;
+    int64_t comp_stride;
+} picasso_particle_field;
+
+/* Grid array: element (i, j, k, comp) at data + i*stride[0] + j*stride[1] +
+ * k*stride[2] + comp*stride[3] (elements).  A Cabana::Grid array (Kokkos
+ * LayoutRight) has stride = {ny*nz*nc, nz*nc, nc, 1}. */
+typedef struct picasso_grid_field {
+    void* data;
+    int32_t dtype;      /* picasso_dtype */
+    int32_t fixed_bits; /* PICASSO_I64_FIXED only: fraction bits (0..62) */
+    int64_t stride[4];
+} picasso_grid_field;
+
+/* Particles sorted by stencil bin in tiles (output of picasso_cell_sort after
+ * the particle arrays were permuted with picasso_permute).  With it the P2G
+ * and G2P entry points use the shared-memory tiled kernels. */
+typedef struct picasso_bins {
+    int32_t tile[3];            /* bins per tile along i, j, k */
+    int32_t num_tiles[3];       /* tiles along i, j, k */
+    int32_t bin_extent[3];      /* bins along i, j, k */
+    int32_t order;              /* spline order the bins were built for */
+    int32_t location;           /* picasso_location the bins were built for */
+    int32_t pad_;
+    const int64_t* tile_offset; /* device, num_tiles_total + 1 particle offsets */
+} picasso_bins;
+
+/* Execution context of one call. */
+typedef struct picasso_exec {
+    void* stream;           /* cudaStream_t; NULL = legacy default stream */
+    int32_t* error_count;   /* optional device int32: particles skipped because
+                               their stencil left a non-periodic mesh */
+    const picasso_bins* bins; /* optional: particles are tile-sorted (see above) */
+} picasso_exec;
+
+/* ------------------------------------------------------------------------ */
+/* Library                                                                  */
+/* ------------------------------------------------------------------------ */
+PICASSO_API const char* picasso_version(void);
+PICASSO_API const char* picasso_status_string(picasso_status s);
+/* Name of the last CUDA error seen by this host thread (or ""). */
+PICASSO_API const char* picasso_last_cuda_error(void);
+
+/* ------------------------------------------------------------------------ */
+/* APIC (Picasso::APIC, src/Picasso_APIC.hpp)                               */
+/* ------------------------------------------------------------------------ */
+
+/* APIC::p2g(m_p, c_p, m_i, mu_i, sd) over num_particles particles.
+ * Replaces Picasso_APIC.hpp:55-140 (collocated, order 2/3), :148-232
+ * (staggered Face/Edge, order 2/3), :240-319 (collocated, order 1) and
+ * :327-402 (staggered, order 1), looped as GridOperator.hpp:612-642 does.
+ * c_p is the 4 x ncomp particle matrix (row 0 = field value, rows 1..3 =
+ * transposed affine matrix).  Collocated locations scatter ncomp components
+ * into mu_i; Face/Edge locations scatter the location's dimension of a
+ * 3-component c_p into component 0 of mu_i.  Results are ADDED to m_i / mu_i
+ * (the reference's ScatterView contribution); zero them first with
+ * picasso_grid_fill to get the GridOperator semantics.
+ * dtypes: plain form: x_p, m_p, c_p, m_i, mu_i all F64 (global FP64 atomics).
+ *         precision form: x_p F64; m_p, c_p F32; m_i, mu_i I64_FIXED
+ *         (deterministic: every contribution is rounded to fixed point).
+ *         F64 particles with I64_FIXED grid is also accepted. */
+PICASSO_API picasso_status picasso_apic_p2g(const picasso_spline* sd, int64_t num_particles,
+                                int32_t ncomp, picasso_particle_field x_p,
+                                picasso_particle_field m_p, picasso_particle_field c_p,
+                                picasso_grid_field m_i, picasso_grid_field mu_i,
+                                const picasso_exec* exec);
+
+/* APIC::g2p(u_i, c_p, sd).  Replaces Picasso_APIC.hpp:407-472 (collocated)
+ * and :477-544 (staggered: writes row `dim` of u_p / B_p, zero elsewhere, as
+ * the reference does).  c_p is overwritten.
+ * dtypes: x_p F64; u_i F64 with c_p F64, or u_i F32 with c_p F32. */
+PICASSO_API picasso_status picasso_apic_g2p(const picasso_spline* sd, int64_t num_particles,
+                                int32_t ncomp, picasso_particle_field x_p,
+                                picasso_grid_field u_i, picasso_particle_field c_p,
+                                const picasso_exec* exec);
+
+/* ------------------------------------------------------------------------ */
+/* PolyPIC (Picasso::PolyPIC, src/Picasso_PolyPIC.hpp)                      */
+/* ------------------------------------------------------------------------ */
+
+/* PolyPIC::p2g(m_p, u_p, c_p, mu_i, m_i, dt, sd) -- note field before mass,
+ * as in the reference.  Linear (order 1, 8 modes) replaces
+ * Picasso_PolyPIC.hpp:39-130 (collocated) and :138-229 (staggered).
+ * Quadratic (order 2, 27 modes) has no reference implementation; see the
+ * library documentation for its definition.  u_p is the 8 (27) x 3 velocity
+ * mode matrix defining the affine material motion, c_p the 8 (27) x ncomp
+ * field modes (u_p == c_p when the field is the velocity).  Adds into mu_i
+ * and m_i. */
+PICASSO_API picasso_status picasso_polypic_p2g(const picasso_spline* sd, int64_t num_particles,
+                                   int32_t ncomp, picasso_particle_field x_p,
+                                   picasso_particle_field m_p, picasso_particle_field u_p,
+                                   picasso_particle_field c_p, picasso_grid_field mu_i,
+                                   picasso_grid_field m_i, double dt,
+                                   const picasso_exec* exec);
+
+/* PolyPIC::g2p(u_i, c_p, sd).  Replaces Picasso_PolyPIC.hpp:235-293
+ * (collocated, c_p overwritten) and :299-358 (staggered: only column `dim`
+ * of c_p is overwritten). */
+PICASSO_API picasso_status picasso_polypic_g2p(const picasso_spline* sd, int64_t num_particles,
+                                   int32_t ncomp, picasso_particle_field x_p,
+                                   picasso_grid_field u_i, picasso_particle_field c_p,
+                                   const picasso_exec* exec);
+
+/* ------------------------------------------------------------------------ */
+/* Grid-side helpers between P2G and G2P                                    */
+/* ------------------------------------------------------------------------ */
+
+/* Set components [0, ncomp) of every entity of the extent[0..2] box of mesh
+ * to `value` (GridOperator.hpp:532-533 zeroes scatter fields this way). */
+PICASSO_API picasso_status picasso_grid_fill(const picasso_mesh* mesh, int32_t ncomp,
+                                 picasso_grid_field f, double value,
+                                 const picasso_exec* exec);
+
+/* Grid velocity update u_i = mu_i / m_i where m_i > mass_threshold, else 0,
+ * on the owned entities (all entities along non-periodic dimensions).  The
+ * division and threshold run in FP64 whatever the storage types; u_i may be
+ * F64 or F32, m_i / mu_i F64 or I64_FIXED.  Optional u64_i (F64, may have
+ * data == NULL) receives the FP64 velocity as well.  No reference
+ * counterpart (the reference leaves the grid update to applications). */
+PICASSO_API picasso_status picasso_grid_velocity(const picasso_mesh* mesh, int32_t ncomp,
+                                     picasso_grid_field m_i, picasso_grid_field mu_i,
+                                     double mass_threshold, picasso_grid_field u_i,
+                                     picasso_grid_field u64_i, const picasso_exec* exec);
+
+/* Particle advection x_p += dt * c_p(0, :) in FP64, then periodic wrap of the
+ * position into the owned box along periodic dimensions. */
+PICASSO_API picasso_status picasso_advect(const picasso_mesh* mesh, int64_t num_particles,
+                              double dt, picasso_particle_field x_p,
+                              picasso_particle_field c_p, const picasso_exec* exec);
+
+/* ------------------------------------------------------------------------ */
+/* Particle cell-sort                                                       */
+/* ------------------------------------------------------------------------ */
+
+/* Bytes of device workspace picasso_cell_sort needs for num_particles
+ * particles and the given spline / tile shape. */
+PICASSO_API picasso_status picasso_cell_sort_workspace(const picasso_spline* sd, int64_t num_particles,
+                                           const int32_t tile[3], int64_t* bytes);
+
+/* Stable sort of the particles by stencil bin in tiles.  The bin of a
+ * particle is the first index of its spline stencil along each dimension
+ * (wrapped into the owned range along periodic dimensions); the key is
+ *   key = tile_linear * (tile[0]*tile[1]*tile[2]) + bin_in_tile_linear
+ * (i slowest, k fastest in both).  A particle whose stencil leaves a
+ * non-periodic mesh gets key = num_tiles * tile volume and sorts last.
+ * Outputs (device): key[num_particles] (sorted keys), perm[num_particles]
+ * (perm[r] = original index of the particle of rank r; ties keep the
+ * original order) and tile_offset[num_tiles + 1] (first rank of each tile;
+ * the last entry counts the particles inside the mesh).  bins_out (host) is
+ * filled for picasso_exec.bins.  workspace: device memory of at least the
+ * size picasso_cell_sort_workspace reports, 256-byte aligned.
+ * No reference counterpart: Picasso has no particle sort. */
+PICASSO_API picasso_status picasso_cell_sort(const picasso_spline* sd, int64_t num_particles,
+                                 picasso_particle_field x_p, const int32_t tile[3],
+                                 uint32_t* key, uint32_t* perm, int64_t* tile_offset,
+                                 void* workspace, int64_t workspace_bytes,
+                                 picasso_bins* bins_out, const picasso_exec* exec);
+
+/* Gather a particle member: dst(p, c) = src(perm[p], c) for c < ncomp.
+ * src and dst must not overlap. */
+PICASSO_API picasso_status picasso_permute(int64_t num_particles, int32_t ncomp, const uint32_t* perm,
+                               picasso_particle_field src, picasso_particle_field dst,
+                               const picasso_exec* exec);
+
+/* ------------------------------------------------------------------------ */
+/* Batched 3x3 linear algebra (LinearAlgebra, BatchedLinearAlgebra.hpp)     */
+/* ------------------------------------------------------------------------ */
+
+/* For each of n row-major 3x3 FP64 matrices a[9*b..]: det[b] = !a
+ * (Picasso_BatchedLinearAlgebra.hpp:4337-4350) and, when a_inv != NULL,
+ * a_inv = inverse(a) by cofactors times 1/det (:4626-4686).  When x != NULL
+ * and y != NULL also y = a_inv * x (3-vectors). */
+PICASSO_API picasso_status picasso_mat3_inverse(int64_t n, const double* a, double* a_inv, double* det,
+                                    const double* x, double* y, const picasso_exec* exec);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PICASSO_B200_H */

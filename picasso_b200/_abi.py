@@ -1,0 +1,142 @@
+"""ctypes mirror of include/picasso_b200.h and the loader of the CUDA library.
+
+The structures here must match the C header field for field; a CPU test
+compiles a small C program that prints sizeof/offsetof of every descriptor
+and compares it with these definitions.
+"""
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpicasso_b200.so")
+
+# status codes
+OK = 0
+ERR_INVALID_ARGUMENT = 1
+ERR_UNSUPPORTED = 2
+ERR_CUDA = 3
+ERR_OUT_OF_RANGE = 4
+ERR_TIMEOUT = 5
+ERR_NO_DEVICE = 6
+
+# dtypes
+F64 = 0
+F32 = 1
+I64_FIXED = 2
+
+# locations
+NODE = 0
+CELL = 1
+FACE_I, FACE_J, FACE_K = 2, 3, 4
+EDGE_I, EDGE_J, EDGE_K = 5, 6, 7
+
+SOA_SHIFT = 62
+
+
+class Mesh(C.Structure):
+    _fields_ = [("extent", C.c_int32 * 3), ("own_begin", C.c_int32 * 3),
+                ("own_extent", C.c_int32 * 3), ("periodic", C.c_int32 * 3),
+                ("low_corner", C.c_double * 3), ("cell_size", C.c_double * 3)]
+
+
+class Spline(C.Structure):
+    _fields_ = [("mesh", Mesh), ("location", C.c_int32), ("order", C.c_int32)]
+
+
+class ParticleField(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("dtype", C.c_int32), ("vector_shift", C.c_int32),
+                ("tile_stride", C.c_int64), ("comp_stride", C.c_int64)]
+
+
+class GridField(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("dtype", C.c_int32), ("fixed_bits", C.c_int32),
+                ("stride", C.c_int64 * 4)]
+
+
+class Bins(C.Structure):
+    _fields_ = [("tile", C.c_int32 * 3), ("num_tiles", C.c_int32 * 3),
+                ("bin_extent", C.c_int32 * 3), ("order", C.c_int32), ("location", C.c_int32),
+                ("pad_", C.c_int32), ("tile_offset", C.c_void_p)]
+
+
+class Exec(C.Structure):
+    _fields_ = [("stream", C.c_void_p), ("error_count", C.c_void_p),
+                ("bins", C.POINTER(Bins))]
+
+
+# (name, restype, argtypes) of every entry point in the header
+SIGNATURES = [
+    ("picasso_version", C.c_char_p, []),
+    ("picasso_status_string", C.c_char_p, [C.c_int]),
+    ("picasso_last_cuda_error", C.c_char_p, []),
+    ("picasso_apic_p2g", C.c_int,
+     [C.POINTER(Spline), C.c_int64, C.c_int32, ParticleField, ParticleField, ParticleField,
+      GridField, GridField, C.POINTER(Exec)]),
+    ("picasso_apic_g2p", C.c_int,
+     [C.POINTER(Spline), C.c_int64, C.c_int32, ParticleField, GridField, ParticleField,
+      C.POINTER(Exec)]),
+    ("picasso_polypic_p2g", C.c_int,
+     [C.POINTER(Spline), C.c_int64, C.c_int32, ParticleField, ParticleField, ParticleField,
+      ParticleField, GridField, GridField, C.c_double, C.POINTER(Exec)]),
+    ("picasso_polypic_g2p", C.c_int,
+     [C.POINTER(Spline), C.c_int64, C.c_int32, ParticleField, GridField, ParticleField,
+      C.POINTER(Exec)]),
+    ("picasso_grid_fill", C.c_int,
+     [C.POINTER(Mesh), C.c_int32, GridField, C.c_double, C.POINTER(Exec)]),
+    ("picasso_grid_velocity", C.c_int,
+     [C.POINTER(Mesh), C.c_int32, GridField, GridField, C.c_double, GridField, GridField,
+      C.POINTER(Exec)]),
+    ("picasso_advect", C.c_int,
+     [C.POINTER(Mesh), C.c_int64, C.c_double, ParticleField, ParticleField, C.POINTER(Exec)]),
+    ("picasso_cell_sort_workspace", C.c_int,
+     [C.POINTER(Spline), C.c_int64, C.POINTER(C.c_int32), C.POINTER(C.c_int64)]),
+    ("picasso_cell_sort", C.c_int,
+     [C.POINTER(Spline), C.c_int64, ParticleField, C.POINTER(C.c_int32), C.c_void_p,
+      C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.POINTER(Bins), C.POINTER(Exec)]),
+    ("picasso_permute", C.c_int,
+     [C.c_int64, C.c_int32, C.c_void_p, ParticleField, ParticleField, C.POINTER(Exec)]),
+    ("picasso_mat3_inverse", C.c_int,
+     [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+      C.POINTER(Exec)]),
+]
+
+_lib = None
+
+
+class PicassoError(RuntimeError):
+    """A C-ABI entry point returned a non-zero status."""
+
+    def __init__(self, status, where):
+        lib = _lib
+        msg = lib.picasso_status_string(status).decode() if lib else str(status)
+        if status == ERR_CUDA and lib:
+            msg += ": " + lib.picasso_last_cuda_error().decode()
+        super().__init__("%s failed: %s (status %d)" % (where, msg, status))
+        self.status = status
+
+
+def load_library(path=None):
+    """Load libpicasso_b200.so (built in-tree by picasso_b200._build).
+
+    Raises ImportError when the library has not been built: there is no
+    fallback implementation."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise ImportError("libpicasso_b200.so not built (%s); run picasso_b200._build.build()" % p)
+    lib = C.CDLL(p)
+    for name, res, args in SIGNATURES:
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def check(status, where):
+    if status != OK:
+        raise PicassoError(status, where)

@@ -1,0 +1,463 @@
+"""Host-side interface mirroring Picasso's transfer API on top of the C ABI.
+
+Reference interfaces (paths inside the Picasso source tree):
+  UniformMesh geometry           src/Picasso_UniformMesh.hpp:73-196
+  FieldLocation / entity types   src/Picasso_FieldTypes.hpp:125-168
+  InterpolationOrder, createSpline
+                                 src/Picasso_ParticleInterpolation.hpp:27-105
+  APIC::p2g / APIC::g2p          src/Picasso_APIC.hpp:55-544
+  PolyPIC::p2g / PolyPIC::g2p    src/Picasso_PolyPIC.hpp:39-359
+  GridOperator scatter zeroing   src/Picasso_GridOperator.hpp:532-533
+
+Particle members are torch CUDA tensors shaped (N,), (N, C) or (N, R, C) with
+any strides whose inner (R, C) block is row-major contiguous; grid arrays are
+torch CUDA tensors shaped (nx, ny, nz) or (nx, ny, nz, C).  A fixed-point grid
+accumulator is a :class:`FixedGrid` (an int64 tensor plus its fraction bits).
+Every call enqueues on the current torch CUDA stream unless ``stream`` is
+given; there is no CPU path.
+"""
+
+import ctypes as C
+import math
+
+import torch
+
+from . import _abi
+from ._abi import check
+
+# ---------------------------------------------------------------------------
+# field locations and orders
+# ---------------------------------------------------------------------------
+
+
+class FieldLocation:
+    """Mesh entity types (Picasso FieldLocation)."""
+
+    Node = _abi.NODE
+    Cell = _abi.CELL
+
+    @staticmethod
+    def Face(dim):
+        if dim not in (0, 1, 2):
+            raise ValueError("Face dimension out of bounds")
+        return _abi.FACE_I + dim
+
+    @staticmethod
+    def Edge(dim):
+        if dim not in (0, 1, 2):
+            raise ValueError("Edge dimension out of bounds")
+        return _abi.EDGE_I + dim
+
+
+def staggered_dim(location):
+    if _abi.FACE_I <= location <= _abi.FACE_K:
+        return location - _abi.FACE_I
+    if _abi.EDGE_I <= location <= _abi.EDGE_K:
+        return location - _abi.EDGE_I
+    return -1
+
+
+def _node_aligned(location, d):
+    """True if the entity sits on nodes along dimension d."""
+    if location == _abi.NODE:
+        return True
+    if location == _abi.CELL:
+        return False
+    s = staggered_dim(location)
+    if location <= _abi.FACE_K:
+        return d == s
+    return d != s
+
+
+class InterpolationOrder(int):
+    """InterpolationOrder<N>: 1 linear, 2 quadratic, 3 cubic."""
+
+    def __new__(cls, n):
+        if n not in (1, 2, 3):
+            raise ValueError("interpolation order must be 1, 2 or 3")
+        return int.__new__(cls, n)
+
+
+# ---------------------------------------------------------------------------
+# mesh
+# ---------------------------------------------------------------------------
+
+
+class UniformMesh:
+    """Single-rank uniform mesh with the geometry conventions of
+    Picasso::UniformMesh: cells from a cell size (or a cell count) over a
+    bounding box, non-periodic dimensions padded by the minimum halo width,
+    a local grid with ``halo_cell_width`` ghost layers on every side whose
+    node (0,0,0) sits at ``low_corner``."""
+
+    def __init__(self, global_bounding_box, cell_size=None, global_num_cell=None,
+                 periodic=(False, False, False), halo_cell_width=0,
+                 minimum_halo_cell_width=0):
+        box = [float(v) for v in global_bounding_box]
+        if len(box) != 6:
+            raise ValueError("bounding box needs 6 entries")
+        if cell_size is not None:
+            cs = float(cell_size)
+            ncell = [int(round((box[d + 3] - box[d]) / cs)) for d in range(3)]
+        elif global_num_cell is not None:
+            ncell = [int(v) for v in global_num_cell]
+            if len(ncell) != 3:
+                raise ValueError("3 entries required for mesh.global_num_cell")
+            cs = (box[3] - box[0]) / ncell[0]
+        else:
+            raise ValueError("Invalid uniform mesh size parameters")
+        for d in range(3):
+            if abs(ncell[d] * cs - (box[d + 3] - box[d])) > 1.1920929e-07:
+                raise ValueError("Extent not evenly divisible by uniform cell size")
+        periodic = [bool(p) for p in periodic]
+        if len(periodic) != 3:
+            raise ValueError("3 entries required for mesh.periodic")
+        low = box[:3]
+        for d in range(3):
+            if not periodic[d]:
+                ncell[d] += 2 * minimum_halo_cell_width
+                low[d] -= cs * minimum_halo_cell_width
+        self.cell_size = cs
+        self.global_num_cell = ncell
+        self.periodic = periodic
+        self.halo_cell_width = max(int(minimum_halo_cell_width), int(halo_cell_width))
+        h = self.halo_cell_width
+        self.global_low_corner = low
+        self.low_corner = [low[d] - h * cs for d in range(3)]
+
+    def owned_extent(self, location, d):
+        n = self.global_num_cell[d]
+        if _node_aligned(location, d) and not self.periodic[d]:
+            return n + 1
+        return n
+
+    def extent(self, location):
+        """Local (ghosted) index extent of the entity arrays of a location."""
+        h = self.halo_cell_width
+        return tuple(self.owned_extent(location, d) + 2 * h for d in range(3))
+
+    def descriptor(self, location):
+        m = _abi.Mesh()
+        ext = self.extent(location)
+        for d in range(3):
+            m.extent[d] = ext[d]
+            m.own_begin[d] = self.halo_cell_width
+            m.own_extent[d] = self.owned_extent(location, d)
+            m.periodic[d] = 1 if self.periodic[d] else 0
+            m.low_corner[d] = self.low_corner[d]
+            m.cell_size[d] = self.cell_size
+        return m
+
+    def zeros(self, location, ncomp=None, dtype=torch.float64, device="cuda"):
+        shape = self.extent(location) + ((ncomp,) if ncomp else ())
+        return torch.zeros(shape, dtype=dtype, device=device)
+
+
+class Spline:
+    """createSpline(Location, InterpolationOrder<N>, mesh, x): the stencil is
+    evaluated inside the transfer kernels from the particle positions."""
+
+    def __init__(self, location, order, mesh, x):
+        self.location = int(location)
+        self.order = int(InterpolationOrder(int(order)))
+        self.mesh = mesh
+        self.x = x
+        self.desc = _abi.Spline()
+        self.desc.mesh = mesh.descriptor(self.location)
+        self.desc.location = self.location
+        self.desc.order = self.order
+
+    @property
+    def num_particles(self):
+        return self.x.shape[0]
+
+
+def create_spline(location, order, mesh, x, *members):
+    """Mirror of Picasso::createSpline; spline members (SplineValue, ...) are
+    accepted and ignored because every member is computed on the fly."""
+    return Spline(location, order, mesh, x)
+
+
+# ---------------------------------------------------------------------------
+# descriptors from tensors
+# ---------------------------------------------------------------------------
+
+_DT = {torch.float64: _abi.F64, torch.float32: _abi.F32}
+
+
+class FixedGrid:
+    """A 64-bit fixed-point grid accumulator: value = raw * 2**-bits."""
+
+    def __init__(self, raw, bits):
+        if raw.dtype != torch.int64:
+            raise TypeError("fixed-point grid must be int64")
+        self.raw = raw
+        self.bits = int(bits)
+
+    def to_float(self, dtype=torch.float64):
+        return self.raw.to(dtype) * (2.0 ** -self.bits)
+
+
+def particle_field(t):
+    """Descriptor of a particle member tensor (N,), (N, C) or (N, R, C)."""
+    if t.dtype not in _DT:
+        raise TypeError("particle members must be float64 or float32")
+    if not t.is_cuda:
+        raise ValueError("particle members must be CUDA tensors")
+    f = _abi.ParticleField()
+    f.data = t.data_ptr()
+    f.dtype = _DT[t.dtype]
+    f.vector_shift = 0
+    f.tile_stride = t.stride(0) if t.dim() >= 1 else 1
+    if t.dim() == 1:
+        f.comp_stride = 0
+    elif t.dim() == 2:
+        f.comp_stride = t.stride(1)
+    elif t.dim() == 3:
+        if t.shape[2] > 1 and t.stride(1) != t.shape[2] * t.stride(2):
+            raise ValueError("matrix members need a row-major (R, C) block")
+        f.comp_stride = t.stride(2) if t.shape[2] > 1 else t.stride(1)
+    else:
+        raise ValueError("particle members are (N,), (N, C) or (N, R, C)")
+    return f
+
+
+def grid_field(t):
+    """Descriptor of a grid tensor (nx, ny, nz[, C]) or a FixedGrid."""
+    g = _abi.GridField()
+    if isinstance(t, FixedGrid):
+        raw = t.raw
+        g.dtype = _abi.I64_FIXED
+        g.fixed_bits = t.bits
+    else:
+        raw = t
+        if raw.dtype not in _DT:
+            raise TypeError("grid arrays must be float64, float32 or a FixedGrid")
+        g.dtype = _DT[raw.dtype]
+        g.fixed_bits = 0
+    if not raw.is_cuda:
+        raise ValueError("grid arrays must be CUDA tensors")
+    if raw.dim() not in (3, 4):
+        raise ValueError("grid arrays are (nx, ny, nz) or (nx, ny, nz, C)")
+    g.data = raw.data_ptr()
+    for d in range(3):
+        g.stride[d] = raw.stride(d)
+    g.stride[3] = raw.stride(3) if raw.dim() == 4 else 0
+    return g
+
+
+def _grid_tensor(t):
+    return t.raw if isinstance(t, FixedGrid) else t
+
+
+def _ncomp_of_grid(t):
+    r = _grid_tensor(t)
+    return r.shape[3] if r.dim() == 4 else 1
+
+
+def _check_grid_extent(t, mesh_desc):
+    r = _grid_tensor(t)
+    for d in range(3):
+        if r.shape[d] < mesh_desc.extent[d]:
+            raise ValueError("grid array smaller than the mesh extent along %d" % d)
+
+
+class Exec:
+    """Execution context: stream, optional skipped-particle counter, bins."""
+
+    def __init__(self, stream=None, error_count=None, bins=None):
+        self.desc = _abi.Exec()
+        s = stream if stream is not None else torch.cuda.current_stream()
+        self.desc.stream = s.cuda_stream if hasattr(s, "cuda_stream") else s
+        self._err = error_count
+        self.desc.error_count = error_count.data_ptr() if error_count is not None else None
+        self._bins = bins
+        self.desc.bins = C.pointer(bins.desc) if bins is not None else None
+
+
+def _exec(stream, error_count, bins):
+    return Exec(stream, error_count, bins)
+
+
+def _lib():
+    return _abi.load_library()
+
+
+# ---------------------------------------------------------------------------
+# APIC
+# ---------------------------------------------------------------------------
+
+
+class APIC:
+    """Picasso::APIC transfers over all particles of the spline."""
+
+    @staticmethod
+    def p2g(m_p, c_p, m_i, mu_i, sd, stream=None, error_count=None, bins=None):
+        """APIC::p2g(m_p, c_p, m_i, mu_i, sd): adds mass and momentum into the
+        grid (zero them first for the GridOperator semantics)."""
+        ncomp = c_p.shape[2]
+        _check_grid_extent(m_i, sd.desc.mesh)
+        _check_grid_extent(mu_i, sd.desc.mesh)
+        ex = _exec(stream, error_count, bins)
+        check(_lib().picasso_apic_p2g(C.byref(sd.desc), sd.num_particles, ncomp,
+                                      particle_field(sd.x), particle_field(m_p),
+                                      particle_field(c_p), grid_field(m_i), grid_field(mu_i),
+                                      C.byref(ex.desc)), "APIC::p2g")
+
+    @staticmethod
+    def g2p(u_i, c_p, sd, stream=None, error_count=None, bins=None):
+        """APIC::g2p(u_i, c_p, sd): overwrites c_p (4 x ncomp per particle)."""
+        ncomp = c_p.shape[2]
+        _check_grid_extent(u_i, sd.desc.mesh)
+        ex = _exec(stream, error_count, bins)
+        check(_lib().picasso_apic_g2p(C.byref(sd.desc), sd.num_particles, ncomp,
+                                      particle_field(sd.x), grid_field(u_i), particle_field(c_p),
+                                      C.byref(ex.desc)), "APIC::g2p")
+
+
+class PolyPIC:
+    """Picasso::PolyPIC transfers (linear 8 modes; quadratic 27 modes)."""
+
+    @staticmethod
+    def p2g(m_p, u_p, c_p, mu_i, m_i, dt, sd, stream=None, error_count=None):
+        """PolyPIC::p2g(m_p, u_p, c_p, mu_i, m_i, dt, sd) -- field before mass."""
+        ncomp = c_p.shape[2]
+        _check_grid_extent(m_i, sd.desc.mesh)
+        _check_grid_extent(mu_i, sd.desc.mesh)
+        ex = _exec(stream, error_count, None)
+        check(_lib().picasso_polypic_p2g(C.byref(sd.desc), sd.num_particles, ncomp,
+                                         particle_field(sd.x), particle_field(m_p),
+                                         particle_field(u_p), particle_field(c_p),
+                                         grid_field(mu_i), grid_field(m_i), float(dt),
+                                         C.byref(ex.desc)), "PolyPIC::p2g")
+
+    @staticmethod
+    def g2p(u_i, c_p, sd, stream=None, error_count=None):
+        """PolyPIC::g2p(u_i, c_p, sd)."""
+        ncomp = c_p.shape[2]
+        _check_grid_extent(u_i, sd.desc.mesh)
+        ex = _exec(stream, error_count, None)
+        check(_lib().picasso_polypic_g2p(C.byref(sd.desc), sd.num_particles, ncomp,
+                                         particle_field(sd.x), grid_field(u_i),
+                                         particle_field(c_p), C.byref(ex.desc)),
+              "PolyPIC::g2p")
+
+
+# ---------------------------------------------------------------------------
+# grid helpers
+# ---------------------------------------------------------------------------
+
+
+def grid_fill(mesh_desc, f, value=0.0, ncomp=None, stream=None):
+    ex = _exec(stream, None, None)
+    nc = ncomp or _ncomp_of_grid(f)
+    check(_lib().picasso_grid_fill(C.byref(mesh_desc), nc, grid_field(f), float(value),
+                                   C.byref(ex.desc)), "grid_fill")
+
+
+def grid_velocity(mesh_desc, m_i, mu_i, u_i, mass_threshold=1e-12, u64_i=None, stream=None):
+    """u_i = mu_i / m_i (FP64 arithmetic) where m_i > threshold, else 0."""
+    ex = _exec(stream, None, None)
+    g64 = grid_field(u64_i) if u64_i is not None else _abi.GridField()
+    check(_lib().picasso_grid_velocity(C.byref(mesh_desc), _ncomp_of_grid(mu_i), grid_field(m_i),
+                                       grid_field(mu_i), float(mass_threshold), grid_field(u_i),
+                                       g64, C.byref(ex.desc)), "grid_velocity")
+
+
+def advect(mesh_desc, x_p, c_p, dt, stream=None):
+    """x_p += dt * c_p(0, :) in FP64 with periodic wrap."""
+    ex = _exec(stream, None, None)
+    v = c_p[:, 0, :] if c_p.dim() == 3 else c_p
+    check(_lib().picasso_advect(C.byref(mesh_desc), x_p.shape[0], float(dt), particle_field(x_p),
+                                particle_field(v), C.byref(ex.desc)), "advect")
+
+
+# ---------------------------------------------------------------------------
+# cell sort
+# ---------------------------------------------------------------------------
+
+
+class Bins:
+    """Result of cell_sort: the C descriptor plus the tensors it points to."""
+
+    def __init__(self, desc, tile_offset):
+        self.desc = desc
+        self.tile_offset = tile_offset
+
+    @property
+    def num_tiles(self):
+        return self.desc.num_tiles[0] * self.desc.num_tiles[1] * self.desc.num_tiles[2]
+
+
+def cell_sort(sd, tile=(8, 8, 8), stream=None, workspace=None):
+    """Stable sort of the spline's particles by (tile, bin).  Returns
+    (key, perm, bins) as uint32-valued int32 / int64 CUDA tensors."""
+    lib = _lib()
+    n = sd.num_particles
+    t3 = (C.c_int32 * 3)(*tile)
+    nbytes = C.c_int64()
+    check(lib.picasso_cell_sort_workspace(C.byref(sd.desc), n, t3, C.byref(nbytes)),
+          "cell_sort_workspace")
+    dev = sd.x.device
+    if workspace is None or workspace.numel() < nbytes.value:
+        workspace = torch.empty(max(nbytes.value, 1), dtype=torch.uint8, device=dev)
+    key = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
+    perm = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
+    nt = 1
+    for d in range(3):
+        m = sd.desc.mesh
+        nb = m.own_extent[d] if m.periodic[d] else m.extent[d]
+        nt *= -(-nb // tile[d])
+    tile_offset = torch.empty(nt + 1, dtype=torch.int64, device=dev)
+    bins = _abi.Bins()
+    ex = _exec(stream, None, None)
+    check(lib.picasso_cell_sort(C.byref(sd.desc), n, particle_field(sd.x), t3, key.data_ptr(),
+                                perm.data_ptr(), tile_offset.data_ptr(), workspace.data_ptr(),
+                                workspace.numel(), C.byref(bins), C.byref(ex.desc)), "cell_sort")
+    return key[:n], perm[:n], Bins(bins, tile_offset)
+
+
+def permute(perm, src, dst=None, stream=None):
+    """dst[p] = src[perm[p]] for a particle member tensor."""
+    if dst is None:
+        dst = torch.empty_like(src)
+    ncomp = 1
+    for s in src.shape[1:]:
+        ncomp *= s
+    ex = _exec(stream, None, None)
+    check(_lib().picasso_permute(src.shape[0], ncomp, perm.data_ptr(), particle_field(src),
+                                 particle_field(dst), C.byref(ex.desc)), "permute")
+    return dst
+
+
+def permute_members(perm, *members, stream=None):
+    return tuple(permute(perm, m, stream=stream) for m in members)
+
+
+# ---------------------------------------------------------------------------
+# 3x3 linear algebra
+# ---------------------------------------------------------------------------
+
+
+def mat3_inverse(a, x=None, stream=None):
+    """Batched (n, 3, 3) FP64 determinant and cofactor inverse; with x (n, 3)
+    also returns inverse(a) @ x."""
+    a = a.contiguous()
+    n = a.shape[0]
+    inv = torch.empty_like(a)
+    det = torch.empty(n, dtype=a.dtype, device=a.device)
+    y = torch.empty_like(x) if x is not None else None
+    ex = _exec(stream, None, None)
+    check(_lib().picasso_mat3_inverse(n, a.data_ptr(), inv.data_ptr(), det.data_ptr(),
+                                      x.contiguous().data_ptr() if x is not None else None,
+                                      y.data_ptr() if y is not None else None, C.byref(ex.desc)),
+          "mat3_inverse")
+    return (inv, det, y) if x is not None else (inv, det)
+
+
+def fixed_bits_for(max_abs):
+    """Largest fraction bit count whose 64-bit fixed point still holds
+    +-max_abs with a factor 4 of headroom."""
+    if max_abs <= 0:
+        return 40
+    return max(0, min(62, 60 - int(math.ceil(math.log2(max_abs)))))

@@ -1,0 +1,211 @@
+// Grid-side operations between P2G and G2P: fill (the GridOperator's zeroing
+// of scatter fields), the FP64 momentum-to-velocity update with the
+// near-empty-node threshold, and the FP64 particle position update.
+#include <cmath>
+
+#include "common.cuh"
+
+namespace pb {
+
+struct Box {
+    int lo[3];
+    int n[3];
+    __host__ __device__ int64_t count() const { return (int64_t)n[0] * n[1] * n[2]; }
+    __device__ __forceinline__ void at(int64_t e, int& i, int& j, int& k) const
+    {
+        k = lo[2] + (int)(e % n[2]);
+        e /= n[2];
+        j = lo[1] + (int)(e % n[1]);
+        i = lo[0] + (int)(e / n[1]);
+    }
+};
+
+static Box full_box(const picasso_mesh& m)
+{
+    Box b;
+    for (int d = 0; d < 3; ++d) {
+        b.lo[d] = 0;
+        b.n[d] = m.extent[d];
+    }
+    return b;
+}
+
+static Box owned_box(const picasso_mesh& m)
+{
+    Box b;
+    for (int d = 0; d < 3; ++d) {
+        b.lo[d] = m.periodic[d] ? m.own_begin[d] : 0;
+        b.n[d] = m.periodic[d] ? m.own_extent[d] : m.extent[d];
+    }
+    return b;
+}
+
+template <class T>
+__global__ void fill_kernel(Box b, GField f, int ncomp, T v)
+{
+    const int64_t total = b.count() * ncomp;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        int i, j, k;
+        b.at(e / ncomp, i, j, k);
+        *f.ptr<T>(i, j, k, (int)(e % ncomp)) = v;
+    }
+}
+
+template <class T>
+__device__ __forceinline__ double load_value(const GField& f, int i, int j, int k, int c,
+                                             double scale_inv)
+{
+    return (double)*f.ptr<T>(i, j, k, c) * scale_inv;
+}
+
+// u = mu / m where m > threshold else 0; all arithmetic in FP64.
+template <class MT, class UT, int NC>
+__global__ void velocity_kernel(Box b, GField gm, GField gmu, GField gu, GField gu64,
+                                double thr, double inv_m, double inv_mu)
+{
+    const int64_t total = b.count();
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        int i, j, k;
+        b.at(e, i, j, k);
+        const double m = load_value<MT>(gm, i, j, k, 0, inv_m);
+        const bool keep = m > thr;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            const double v = keep ? load_value<MT>(gmu, i, j, k, c, inv_mu) / m : 0.0;
+            *gu.ptr<UT>(i, j, k, c) = (UT)v;
+            if (gu64.data) *gu64.ptr<double>(i, j, k, c) = v;
+        }
+    }
+}
+
+template <class MT, class UT>
+static void launch_velocity(int ncomp, Box b, GField gm, GField gmu, GField gu, GField gu64,
+                            double thr, double inv_m, double inv_mu, cudaStream_t st)
+{
+    const unsigned blocks = grid_for(b.count(), 256, 148LL * 32);
+    if (ncomp == 1)
+        velocity_kernel<MT, UT, 1><<<blocks, 256, 0, st>>>(b, gm, gmu, gu, gu64, thr, inv_m, inv_mu);
+    else if (ncomp == 2)
+        velocity_kernel<MT, UT, 2><<<blocks, 256, 0, st>>>(b, gm, gmu, gu, gu64, thr, inv_m, inv_mu);
+    else
+        velocity_kernel<MT, UT, 3><<<blocks, 256, 0, st>>>(b, gm, gmu, gu, gu64, thr, inv_m, inv_mu);
+}
+
+template <class CT>
+__global__ void advect_kernel(int64_t n, PField x, PField c, double dt, int3 periodic,
+                              double3 lo, double3 len)
+{
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
+         p += (int64_t)gridDim.x * blockDim.x) {
+        const int per[3] = {periodic.x, periodic.y, periodic.z};
+        const double l0[3] = {lo.x, lo.y, lo.z};
+        const double ln[3] = {len.x, len.y, len.z};
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            double xn = x.get<double>(p, d) + dt * (double)c.get<CT>(p, d);
+            if (per[d]) {
+                if (xn < l0[d]) xn += ln[d];
+                else if (xn >= l0[d] + ln[d]) xn -= ln[d];
+            }
+            x.set<double>(p, d, xn);
+        }
+    }
+}
+
+}  // namespace pb
+
+using namespace pb;
+
+extern "C" picasso_status picasso_grid_fill(const picasso_mesh* mesh, int32_t ncomp,
+                                            picasso_grid_field f, double value,
+                                            const picasso_exec* exec)
+{
+    picasso_status st = validate_mesh(mesh);
+    if (st) return st;
+    if (ncomp < 1) return PICASSO_ERR_INVALID_ARGUMENT;
+    if ((st = validate_gfield(f, PICASSO_F64, PICASSO_F32)) &&
+        (st = validate_gfield(f, PICASSO_I64_FIXED)))
+        return st;
+    Box b = full_box(*mesh);
+    GField g = make_gfield(f);
+    cudaStream_t s = stream_of(exec);
+    const unsigned blocks = grid_for(b.count() * ncomp, 256, 148LL * 32);
+    if (f.dtype == PICASSO_F64)
+        fill_kernel<double><<<blocks, 256, 0, s>>>(b, g, ncomp, value);
+    else if (f.dtype == PICASSO_F32)
+        fill_kernel<float><<<blocks, 256, 0, s>>>(b, g, ncomp, (float)value);
+    else
+        fill_kernel<long long><<<blocks, 256, 0, s>>>(b, g, ncomp,
+                                                      llrint(ldexp(value, f.fixed_bits)));
+    return check_launch();
+}
+
+extern "C" picasso_status picasso_grid_velocity(const picasso_mesh* mesh, int32_t ncomp,
+                                                picasso_grid_field m_i, picasso_grid_field mu_i,
+                                                double mass_threshold, picasso_grid_field u_i,
+                                                picasso_grid_field u64_i,
+                                                const picasso_exec* exec)
+{
+    picasso_status st = validate_mesh(mesh);
+    if (st) return st;
+    if (ncomp < 1 || ncomp > 3) return PICASSO_ERR_INVALID_ARGUMENT;
+    if ((st = validate_gfield(m_i, PICASSO_F64, PICASSO_I64_FIXED))) return st;
+    if ((st = validate_gfield(mu_i, m_i.dtype))) return st;
+    if ((st = validate_gfield(u_i, PICASSO_F64, PICASSO_F32))) return st;
+    if (u64_i.data && (st = validate_gfield(u64_i, PICASSO_F64))) return st;
+    Box b = owned_box(*mesh);
+    GField gm = make_gfield(m_i), gmu = make_gfield(mu_i), gu = make_gfield(u_i);
+    GField gu64 = make_gfield(u64_i);
+    cudaStream_t s = stream_of(exec);
+    const bool fixed = m_i.dtype == PICASSO_I64_FIXED;
+    const double inv_m = fixed ? ldexp(1.0, -m_i.fixed_bits) : 1.0;
+    const double inv_mu = fixed ? ldexp(1.0, -mu_i.fixed_bits) : 1.0;
+    if (fixed) {
+        if (u_i.dtype == PICASSO_F32)
+            launch_velocity<long long, float>(ncomp, b, gm, gmu, gu, gu64, mass_threshold, inv_m,
+                                              inv_mu, s);
+        else
+            launch_velocity<long long, double>(ncomp, b, gm, gmu, gu, gu64, mass_threshold,
+                                               inv_m, inv_mu, s);
+    } else {
+        if (u_i.dtype == PICASSO_F32)
+            launch_velocity<double, float>(ncomp, b, gm, gmu, gu, gu64, mass_threshold, inv_m,
+                                           inv_mu, s);
+        else
+            launch_velocity<double, double>(ncomp, b, gm, gmu, gu, gu64, mass_threshold, inv_m,
+                                            inv_mu, s);
+    }
+    return check_launch();
+}
+
+extern "C" picasso_status picasso_advect(const picasso_mesh* mesh, int64_t num_particles,
+                                         double dt, picasso_particle_field x_p,
+                                         picasso_particle_field c_p, const picasso_exec* exec)
+{
+    picasso_status st = validate_mesh(mesh);
+    if (st) return st;
+    if (num_particles < 0) return PICASSO_ERR_INVALID_ARGUMENT;
+    if ((st = validate_pfield(x_p, PICASSO_F64))) return st;
+    if ((st = validate_pfield(c_p, PICASSO_F64, PICASSO_F32))) return st;
+    if (num_particles == 0) return PICASSO_OK;
+    PField x = make_pfield(x_p), c = make_pfield(c_p);
+    int3 per = make_int3(mesh->periodic[0] != 0, mesh->periodic[1] != 0, mesh->periodic[2] != 0);
+    double l[3], n[3];
+    for (int d = 0; d < 3; ++d) {
+        l[d] = mesh->low_corner[d] + mesh->own_begin[d] * mesh->cell_size[d];
+        n[d] = mesh->own_extent[d] * mesh->cell_size[d];
+    }
+    cudaStream_t s = stream_of(exec);
+    const unsigned blocks = grid_for(num_particles, 256);
+    if (c_p.dtype == PICASSO_F64)
+        advect_kernel<double><<<blocks, 256, 0, s>>>(num_particles, x, c, dt, per,
+                                                     make_double3(l[0], l[1], l[2]),
+                                                     make_double3(n[0], n[1], n[2]));
+    else
+        advect_kernel<float><<<blocks, 256, 0, s>>>(num_particles, x, c, dt, per,
+                                                    make_double3(l[0], l[1], l[2]),
+                                                    make_double3(n[0], n[1], n[2]));
+    return check_launch();
+}

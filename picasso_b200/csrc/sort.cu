@@ -1,0 +1,433 @@
+// Particle cell-sort: key = (tile, bin in tile) of the particle's stencil
+// start, then a stable LSD radix sort of (key, particle index) pairs, then
+// per-tile particle offsets.  Also the member gather used to apply the
+// permutation to particle storage.
+//
+// Radix pass (digit width <= 9 bits): a histogram kernel counts the digits
+// of each 2048-element block, a device-wide exclusive scan turns the
+// digit-major [digit][block] count table into output offsets, and the
+// scatter kernel ranks each element among equal digits of its block in
+// original order (warp __match_any_sync + a per-warp running count, then a
+// prefix over the block's warps), so every pass is stable.
+#include <cmath>
+
+#include "common.cuh"
+
+namespace pb {
+
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 8;
+constexpr int kSortTile = kSortThreads * kSortItems;  // elements per block
+constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kMaxDigitBits = 9;
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 4;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+struct BinP {
+    MeshP mp;
+    int order;
+    int tile[3];
+    int nt[3];
+    int nb[3];
+    uint32_t tsize;
+    uint32_t nkeys;  // valid keys are < nkeys; out-of-mesh particles get nkeys
+};
+
+__device__ __forceinline__ uint32_t particle_key(const BinP& bp, const double xs[3])
+{
+    const int K = bp.order + 1;
+    const int first = (bp.order == 1) ? 0 : -1;
+    const double shift = (bp.order == 2) ? 0.5 : 0.0;
+    int b[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const double x0 = logical_coord(xs[d], bp.mp.lo[d], bp.mp.rdx[d], shift);
+        const int s = (int)floor(x0) + first;
+        if (bp.mp.periodic[d]) {
+            int r = (s - bp.mp.own_lo[d]) % bp.nb[d];
+            if (r < 0) r += bp.nb[d];
+            b[d] = r;
+        } else {
+            if (s < 0 || s + K > bp.mp.ext[d]) return bp.nkeys;
+            b[d] = s;
+        }
+    }
+    const uint32_t tl = ((uint32_t)(b[0] / bp.tile[0]) * bp.nt[1] + (uint32_t)(b[1] / bp.tile[1])) *
+                            bp.nt[2] +
+                        (uint32_t)(b[2] / bp.tile[2]);
+    const uint32_t ll = ((uint32_t)(b[0] % bp.tile[0]) * bp.tile[1] + (uint32_t)(b[1] % bp.tile[1])) *
+                            bp.tile[2] +
+                        (uint32_t)(b[2] % bp.tile[2]);
+    return tl * bp.tsize + ll;
+}
+
+__global__ void key_kernel(BinP bp, int64_t n, PField x, uint32_t* __restrict__ keys,
+                           uint32_t* __restrict__ vals)
+{
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
+         p += (int64_t)gridDim.x * blockDim.x) {
+        const double xs[3] = {x.get<double>(p, 0), x.get<double>(p, 1), x.get<double>(p, 2)};
+        keys[p] = particle_key(bp, xs);
+        vals[p] = (uint32_t)p;
+    }
+}
+
+__global__ void __launch_bounds__(kSortThreads)
+radix_hist_kernel(const uint32_t* __restrict__ keys, int64_t n, int shift, int bits,
+                  uint32_t* __restrict__ hist, int64_t nblk)
+{
+    __shared__ uint32_t cnt[1 << kMaxDigitBits];
+    const int nd = 1 << bits;
+    const uint32_t mask = (uint32_t)nd - 1;
+    for (int i = threadIdx.x; i < nd; i += kSortThreads) cnt[i] = 0;
+    __syncthreads();
+    const int64_t base = (int64_t)blockIdx.x * kSortTile;
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int r = 0; r < kSortItems; ++r) {
+        const int64_t e = base + (int64_t)r * kSortThreads + threadIdx.x;
+        const bool valid = e < n;
+        const uint32_t dig = valid ? (__ldg(keys + e) >> shift) & mask : 0xFFFFFFFFu;
+        const unsigned peers = __match_any_sync(0xFFFFFFFFu, dig);
+        if (valid && lane == __ffs(peers) - 1) atomicAdd(&cnt[dig], (uint32_t)__popc(peers));
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < nd; i += kSortThreads) hist[(int64_t)i * nblk + blockIdx.x] = cnt[i];
+}
+
+__global__ void __launch_bounds__(kSortThreads)
+radix_scatter_kernel(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
+                     uint32_t* __restrict__ kout, uint32_t* __restrict__ vout, int64_t n,
+                     int shift, int bits, const uint32_t* __restrict__ offs, int64_t nblk)
+{
+    __shared__ uint32_t wcnt[kSortWarps][1 << kMaxDigitBits];
+    const int nd = 1 << bits;
+    const uint32_t mask = (uint32_t)nd - 1;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int i = threadIdx.x; i < kSortWarps * (1 << kMaxDigitBits); i += kSortThreads)
+        (&wcnt[0][0])[i] = 0;
+    __syncthreads();
+    const int64_t base = (int64_t)blockIdx.x * kSortTile + (int64_t)warp * 32 * kSortItems;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    uint32_t key[kSortItems], val[kSortItems], rank[kSortItems];
+#pragma unroll
+    for (int r = 0; r < kSortItems; ++r) {
+        const int64_t e = base + r * 32 + lane;
+        const bool valid = e < n;
+        key[r] = valid ? __ldg(kin + e) : 0u;
+        val[r] = valid ? __ldg(vin + e) : 0u;
+        const uint32_t dig = valid ? (key[r] >> shift) & mask : 0xFFFFFFFFu;
+        const unsigned peers = __match_any_sync(0xFFFFFFFFu, dig);
+        uint32_t cur = 0;
+        if (valid) cur = wcnt[warp][dig];
+        __syncwarp();
+        rank[r] = cur + (uint32_t)__popc(peers & lt_mask);
+        if (valid && lane == 31 - __clz(peers)) wcnt[warp][dig] = cur + (uint32_t)__popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    // per digit: block offset from the scanned table, then exclusive prefix
+    // over the warps in warp order
+    for (int d = threadIdx.x; d < nd; d += kSortThreads) {
+        uint32_t run = offs[(int64_t)d * nblk + blockIdx.x];
+#pragma unroll
+        for (int w = 0; w < kSortWarps; ++w) {
+            const uint32_t t = wcnt[w][d];
+            wcnt[w][d] = run;
+            run += t;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kSortItems; ++r) {
+        const int64_t e = base + r * 32 + lane;
+        if (e < n) {
+            const uint32_t pos = wcnt[warp][(key[r] >> shift) & mask] + rank[r];
+            kout[pos] = key[r];
+            vout[pos] = val[r];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// exclusive scan of a uint32 array (three phases)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* warp_sums,
+                                                         uint32_t* total)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, inc, o);
+        if (lane >= o) inc += t;
+    }
+    if (lane == 31) warp_sums[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = blockDim.x >> 5;
+        uint32_t s = lane < nw ? warp_sums[lane] : 0u;
+        uint32_t si = s;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, si, o);
+            if (lane >= o) si += t;
+        }
+        if (lane < nw) warp_sums[lane] = si - s;
+        if (lane == 31) *total = si;
+    }
+    __syncthreads();
+    const uint32_t r = warp_sums[warp] + inc - v;
+    __syncthreads();
+    return r;
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+scan_reduce_kernel(const uint32_t* __restrict__ in, int64_t m, uint32_t* __restrict__ sums)
+{
+    __shared__ uint32_t red[kScanThreads / 32];
+    const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+    uint32_t s = 0;
+#pragma unroll
+    for (int q = 0; q < kScanItems; ++q)
+        if (base + q < m) s += in[base + q];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xFFFFFFFFu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        uint32_t t = red[threadIdx.x];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xFFFFFFFFu, t, o);
+        if (threadIdx.x == 0) sums[blockIdx.x] = t;
+    }
+}
+
+// Single block: exclusive scan of the block sums in place.
+__global__ void __launch_bounds__(kScanThreads) scan_sums_kernel(uint32_t* sums, int64_t nb)
+{
+    __shared__ uint32_t ws[32];
+    __shared__ uint32_t total;
+    uint32_t carry = 0;
+    for (int64_t base = 0; base < nb; base += kScanThreads) {
+        const int64_t e = base + threadIdx.x;
+        const uint32_t v = e < nb ? sums[e] : 0u;
+        const uint32_t ex = block_exclusive_scan(v, ws, &total);
+        if (e < nb) sums[e] = carry + ex;
+        carry += total;
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+scan_apply_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, int64_t m,
+                  const uint32_t* __restrict__ sums)
+{
+    __shared__ uint32_t ws[32];
+    __shared__ uint32_t total;
+    const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+    uint32_t v[kScanItems];
+    uint32_t s = 0;
+#pragma unroll
+    for (int q = 0; q < kScanItems; ++q) {
+        v[q] = (base + q < m) ? in[base + q] : 0u;
+        s += v[q];
+    }
+    uint32_t run = block_exclusive_scan(s, ws, &total) + sums[blockIdx.x];
+#pragma unroll
+    for (int q = 0; q < kScanItems; ++q) {
+        if (base + q < m) out[base + q] = run;
+        run += v[q];
+    }
+}
+
+__global__ void tile_offset_kernel(const uint32_t* __restrict__ keys, int64_t n, int64_t ntiles,
+                                   uint32_t tsize, int64_t* __restrict__ tile_offset)
+{
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t <= ntiles;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const uint64_t target = (uint64_t)t * tsize;
+        int64_t lo = 0, hi = n;
+        while (lo < hi) {
+            const int64_t mid = (lo + hi) >> 1;
+            if ((uint64_t)keys[mid] < target) lo = mid + 1;
+            else hi = mid;
+        }
+        tile_offset[t] = lo;
+    }
+}
+
+template <class T>
+__global__ void permute_kernel(int64_t n, int ncomp, const uint32_t* __restrict__ perm, PField src,
+                               PField dst)
+{
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
+         p += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t q = perm[p];
+        for (int c = 0; c < ncomp; ++c) dst.set<T>(p, c, src.get<T>(q, c));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+struct SortPlan {
+    BinP bp;
+    int64_t ntiles;
+    int bits, passes, width;
+    int64_t nblk, hist_len, scan_blocks;
+    int64_t off_keys, off_vals, off_hist, off_scan, off_sums, bytes;
+};
+
+static int64_t align256(int64_t v) { return (v + 255) & ~int64_t(255); }
+
+static picasso_status make_plan(const picasso_spline* sd, int64_t n, const int32_t tile[3],
+                                SortPlan* pl)
+{
+    picasso_status st = make_mesh(sd, &pl->bp.mp);
+    if (st) return st;
+    if (!tile || n < 0 || n > 0xFFFFFFFELL) return PICASSO_ERR_INVALID_ARGUMENT;
+    pl->bp.order = sd->order;
+    int64_t nt_total = 1, tsize = 1;
+    for (int d = 0; d < 3; ++d) {
+        if (tile[d] < 1) return PICASSO_ERR_INVALID_ARGUMENT;
+        pl->bp.tile[d] = tile[d];
+        pl->bp.nb[d] = sd->mesh.periodic[d] ? sd->mesh.own_extent[d] : sd->mesh.extent[d];
+        pl->bp.nt[d] = (pl->bp.nb[d] + tile[d] - 1) / tile[d];
+        nt_total *= pl->bp.nt[d];
+        tsize *= tile[d];
+    }
+    const int64_t nkeys = nt_total * tsize;
+    if (nkeys >= 0xFFFFFFFFLL) return PICASSO_ERR_OUT_OF_RANGE;
+    pl->bp.tsize = (uint32_t)tsize;
+    pl->bp.nkeys = (uint32_t)nkeys;
+    pl->ntiles = nt_total;
+    int bits = 1;
+    while ((int64_t(1) << bits) <= nkeys) ++bits;  // keys are in [0, nkeys]
+    pl->bits = bits;
+    pl->passes = (bits + kMaxDigitBits - 1) / kMaxDigitBits;
+    pl->width = (bits + pl->passes - 1) / pl->passes;
+    pl->nblk = (n + kSortTile - 1) / kSortTile;
+    if (pl->nblk < 1) pl->nblk = 1;
+    pl->hist_len = (int64_t(1) << pl->width) * pl->nblk;
+    pl->scan_blocks = (pl->hist_len + kScanTile - 1) / kScanTile;
+    int64_t o = 0;
+    pl->off_keys = o;
+    o = align256(o + 4 * (n > 0 ? n : 1));
+    pl->off_vals = o;
+    o = align256(o + 4 * (n > 0 ? n : 1));
+    pl->off_hist = o;
+    o = align256(o + 4 * pl->hist_len);
+    pl->off_scan = o;
+    o = align256(o + 4 * pl->hist_len);
+    pl->off_sums = o;
+    o = align256(o + 4 * pl->scan_blocks);
+    pl->bytes = o;
+    return PICASSO_OK;
+}
+
+}  // namespace pb
+
+using namespace pb;
+
+extern "C" picasso_status picasso_cell_sort_workspace(const picasso_spline* sd,
+                                                      int64_t num_particles,
+                                                      const int32_t tile[3], int64_t* bytes)
+{
+    if (!bytes) return PICASSO_ERR_INVALID_ARGUMENT;
+    SortPlan pl;
+    picasso_status st = make_plan(sd, num_particles, tile, &pl);
+    if (st) return st;
+    *bytes = pl.bytes;
+    return PICASSO_OK;
+}
+
+extern "C" picasso_status picasso_cell_sort(const picasso_spline* sd, int64_t num_particles,
+                                            picasso_particle_field x_p, const int32_t tile[3],
+                                            uint32_t* key, uint32_t* perm, int64_t* tile_offset,
+                                            void* workspace, int64_t workspace_bytes,
+                                            picasso_bins* bins_out, const picasso_exec* exec)
+{
+    SortPlan pl;
+    picasso_status st = make_plan(sd, num_particles, tile, &pl);
+    if (st) return st;
+    if ((st = validate_pfield(x_p, PICASSO_F64))) return st;
+    if (!key || !perm || !tile_offset || !workspace || workspace_bytes < pl.bytes)
+        return PICASSO_ERR_INVALID_ARGUMENT;
+    if (reinterpret_cast<uintptr_t>(workspace) % 256) return PICASSO_ERR_INVALID_ARGUMENT;
+    const int64_t n = num_particles;
+    cudaStream_t s = stream_of(exec);
+    char* ws = static_cast<char*>(workspace);
+    uint32_t* wk = reinterpret_cast<uint32_t*>(ws + pl.off_keys);
+    uint32_t* wv = reinterpret_cast<uint32_t*>(ws + pl.off_vals);
+    uint32_t* hist = reinterpret_cast<uint32_t*>(ws + pl.off_hist);
+    uint32_t* scan = reinterpret_cast<uint32_t*>(ws + pl.off_scan);
+    uint32_t* sums = reinterpret_cast<uint32_t*>(ws + pl.off_sums);
+    // ping-pong so that the last pass writes the caller's arrays
+    uint32_t *ka = wk, *va = wv, *kb = key, *vb = perm;
+    if (pl.passes % 2 == 0) {
+        ka = key;
+        va = perm;
+        kb = wk;
+        vb = wv;
+    }
+    if (n > 0) {
+        key_kernel<<<grid_for(n, 256), 256, 0, s>>>(pl.bp, n, make_pfield(x_p), ka, va);
+        for (int pass = 0; pass < pl.passes; ++pass) {
+            const int shift = pass * pl.width;
+            const int bits = (shift + pl.width <= pl.bits) ? pl.width : pl.bits - shift;
+            radix_hist_kernel<<<(unsigned)pl.nblk, kSortThreads, 0, s>>>(ka, n, shift, bits, hist,
+                                                                          pl.nblk);
+            const int64_t m = (int64_t(1) << bits) * pl.nblk;
+            const int64_t sb = (m + kScanTile - 1) / kScanTile;
+            scan_reduce_kernel<<<(unsigned)sb, kScanThreads, 0, s>>>(hist, m, sums);
+            scan_sums_kernel<<<1, kScanThreads, 0, s>>>(sums, sb);
+            scan_apply_kernel<<<(unsigned)sb, kScanThreads, 0, s>>>(hist, scan, m, sums);
+            radix_scatter_kernel<<<(unsigned)pl.nblk, kSortThreads, 0, s>>>(
+                ka, va, kb, vb, n, shift, bits, scan, pl.nblk);
+            uint32_t* t = ka;
+            ka = kb;
+            kb = t;
+            t = va;
+            va = vb;
+            vb = t;
+        }
+    }
+    tile_offset_kernel<<<grid_for(pl.ntiles + 1, 256), 256, 0, s>>>(key, n, pl.ntiles, pl.bp.tsize,
+                                                                     tile_offset);
+    if ((st = check_launch())) return st;
+    if (bins_out) {
+        for (int d = 0; d < 3; ++d) {
+            bins_out->tile[d] = pl.bp.tile[d];
+            bins_out->num_tiles[d] = pl.bp.nt[d];
+            bins_out->bin_extent[d] = pl.bp.nb[d];
+        }
+        bins_out->order = sd->order;
+        bins_out->location = sd->location;
+        bins_out->pad_ = 0;
+        bins_out->tile_offset = tile_offset;
+    }
+    return PICASSO_OK;
+}
+
+extern "C" picasso_status picasso_permute(int64_t num_particles, int32_t ncomp,
+                                          const uint32_t* perm, picasso_particle_field src,
+                                          picasso_particle_field dst, const picasso_exec* exec)
+{
+    if (num_particles < 0 || ncomp < 1 || !perm) return PICASSO_ERR_INVALID_ARGUMENT;
+    picasso_status st;
+    if ((st = validate_pfield(src, PICASSO_F64, PICASSO_F32))) return st;
+    if ((st = validate_pfield(dst, src.dtype))) return st;
+    if (src.data == dst.data) return PICASSO_ERR_INVALID_ARGUMENT;
+    if (num_particles == 0) return PICASSO_OK;
+    cudaStream_t s = stream_of(exec);
+    const unsigned blocks = grid_for(num_particles, 256);
+    if (src.dtype == PICASSO_F64)
+        permute_kernel<double><<<blocks, 256, 0, s>>>(num_particles, ncomp, perm, make_pfield(src),
+                                                      make_pfield(dst));
+    else
+        permute_kernel<float><<<blocks, 256, 0, s>>>(num_particles, ncomp, perm, make_pfield(src),
+                                                     make_pfield(dst));
+    return check_launch();
+}
