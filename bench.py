@@ -1,0 +1,476 @@
+#!/usr/bin/env python
+"""Benchmark of the APIC transfer step: P2G -> grid velocity update -> G2P.
+
+Default workload: 256^3 periodic grid, 8 particles per cell (134,217,728
+particles), quadratic B-spline on nodes, clustered positions (70 % of the
+particles in 32 Gaussian blobs of sigma = 2 dx, 30 % uniform), particles
+already cell-sorted and resident in HBM.  One step = zero the grid
+accumulators, P2G, FP64 velocity update (u = p / m where m > 1e-12), G2P.
+
+The headline `value` is the FP32 precision form (FP32 particle state and
+arithmetic, 64-bit fixed-point grid accumulation, FP64 division and
+positions); the plain FP64 form runs on the same particles and is reported
+in `fp64_plain`.  The cell sort and the permutation of particle storage are
+timed separately (`sort`).  `e2e` is the same step through the C ABI with
+the particle arrays in pinned host memory, copies included.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank runs its own replica of the workload (no
+collective in the data path); `value` is the sum over ranks of particles
+divided by the slowest rank's time.
+"""
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = ("P2G+G2P particles/s at 256³·8ppc, FP32 form vs FP64 plain, % HBM roofline")
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--grid", type=int, default=256)
+    ap.add_argument("--ppc", type=int, default=8)
+    ap.add_argument("--order", type=int, default=2)
+    ap.add_argument("--workload", default="clustered", choices=["clustered", "uniform"])
+    ap.add_argument("--tile", type=int, nargs=3, default=[4, 8, 8])
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 plain leg")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--unsorted", action="store_true",
+                    help="keep the generated particle order (plain kernels)")
+    ap.add_argument("--cpu-sample-grid", type=int, default=64)
+    ap.add_argument("--json-out", default=None)
+    return ap.parse_args()
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": PEAKS_FALLBACK["hbm_gbs"], "source": "fallback"}
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+class Clocks:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.path = tempfile.mktemp(suffix=".csv")
+        self.proc = None
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for n, v in zip(names, parts[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the oracle port of the reference's CPU path
+# ---------------------------------------------------------------------------
+def cpu_sample(args, steps, warmup, nthreads):
+    """P2G -> velocity -> G2P of the CPU port (OpenMP, duplicated scatter
+    grids as Kokkos' OpenMP ScatterView) on a bounded sample: the same
+    workload generator on a grid^3 periodic box (grid = --cpu-sample-grid)."""
+    import numpy as np
+    import torch
+
+    import oracle
+    from picasso_b200 import FieldLocation, UniformMesh, create_spline, workloads
+
+    n = args.cpu_sample_grid
+    mesh = UniformMesh([0, 0, 0, 1, 1, 1], cell_size=1.0 / n, periodic=(True, True, True))
+    x = workloads.positions(args.workload, n, args.ppc, seed=1002, device="cpu").numpy()
+    m, c = workloads.particle_state(x.shape[0], seed=1002, device="cpu")
+    m, c = m.numpy(), np.ascontiguousarray(c.numpy())
+    sd = create_spline(FieldLocation.Node, args.order, mesh, None).desc
+    times = []
+    for s in range(warmup + steps):
+        cc = c.copy()
+        t0 = time.perf_counter()
+        oracle.apic_step_omp(sd, x, m, cc, nthreads)
+        t1 = time.perf_counter()
+        if s >= warmup:
+            times.append(t1 - t0)
+    sec = sum(times) / len(times)
+    return {"value": x.shape[0] / sec, "unit": "particles/s", "cores": nthreads, "kind": "port",
+            "sample": "%d^3 periodic grid, %d ppc (%d particles), order %d, %s positions, "
+                      "FP64, OpenMP with duplicated scatter grids; mean of %d steps"
+                      % (n, args.ppc, x.shape[0], args.order, args.workload, steps),
+            "ms_per_step": 1e3 * sec}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return
+    nthreads = os.cpu_count() or 1
+    cb = cpu_sample(args, max(1, args.steps), max(0, args.warmup), nthreads)
+    line = {"metric": METRIC, "value": cb["value"], "unit": "particles/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": cb["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": config_of(args),
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": cb["value"], "unit": "particles/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def config_of(args):
+    return {"workload": "APIC order-%d P2G + FP64 grid velocity + G2P, %d^3 periodic nodes, "
+                        "%d ppc, %s positions, cell-sorted, resident in HBM"
+                        % (args.order, args.grid, args.ppc, args.workload),
+            "grid": args.grid, "ppc": args.ppc, "order": args.order,
+            "particles": args.grid ** 3 * args.ppc, "positions": args.workload,
+            "tile": list(args.tile), "l2": "inputs >> 126 MB L2 (no flush needed)",
+            "parallelism": "replicas"}
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+class Step:
+    """Buffers and launches of one form of the APIC step."""
+
+    def __init__(self, form, mesh, x, m, c, bins, stream):
+        import torch
+
+        import picasso_b200 as pb
+
+        self.pb = pb
+        self.form = form
+        self.mesh = mesh
+        self.loc = pb.FieldLocation.Node
+        self.desc = mesh.descriptor(self.loc)
+        self.sd = pb.create_spline(self.loc, ORDER[0], mesh, x)
+        self.m, self.c = m, c
+        self.bins = bins
+        self.stream = stream
+        ext = mesh.extent(self.loc)
+        dev = x.device
+        if form == "fp32":
+            self.acc = torch.zeros(ext + (4,), dtype=torch.int64, device=dev)
+            self.gm = pb.FixedGrid(self.acc[..., 0], FIXED_BITS)
+            self.gmu = pb.FixedGrid(self.acc[..., 1:], FIXED_BITS)
+            self.u = torch.zeros(ext + (3,), dtype=torch.float32, device=dev)
+        else:
+            self.acc = torch.zeros(ext + (4,), dtype=torch.float64, device=dev)
+            self.gm = self.acc[..., 0]
+            self.gmu = self.acc[..., 1:]
+            self.u = torch.zeros(ext + (3,), dtype=torch.float64, device=dev)
+        self.acc_fill = pb.FixedGrid(self.acc, FIXED_BITS) if form == "fp32" else self.acc
+        self.launches_per_step = 4
+
+    def run(self, events=None):
+        pb = self.pb
+        s = self.stream
+        if events is not None:
+            events[0].record(s)
+        pb.grid_fill(self.desc, self.acc_fill, 0.0, ncomp=4, stream=s)
+        if events is not None:
+            events[1].record(s)
+        pb.APIC.p2g(self.m, self.c, self.gm, self.gmu, self.sd, stream=s, bins=self.bins)
+        if events is not None:
+            events[2].record(s)
+        pb.grid_velocity(self.desc, self.gm, self.gmu, self.u, 1e-12, stream=s)
+        if events is not None:
+            events[3].record(s)
+        pb.APIC.g2p(self.u, self.c, self.sd, stream=s, bins=self.bins)
+        if events is not None:
+            events[4].record(s)
+
+    def kernel_bytes(self, n, nodes):
+        """Algorithmic bytes per launch: fill, p2g, velocity, g2p."""
+        if self.form == "fp32":
+            sf, sg, su = 4, 8, 4
+        else:
+            sf, sg, su = 8, 8, 8
+        sx = 8
+        return {"fill": nodes * 4 * sg,
+                "p2g": n * (3 * sx + 13 * sf) + nodes * 4 * sg,
+                "velocity": nodes * (4 * sg + 3 * su),
+                "g2p": n * (3 * sx + 12 * sf) + nodes * 3 * su}
+
+
+ORDER = [2]
+FIXED_BITS = 36
+
+
+def time_form(step, steps, warmup, dist):
+    import torch
+    names = ["fill", "p2g", "velocity", "g2p"]
+    for _ in range(warmup):
+        step.run()
+    torch.cuda.synchronize()
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(5)] for _ in range(steps)]
+    if dist:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(step.stream)
+    for k in range(steps):
+        step.run(ev[k])
+    t1.record(step.stream)
+    torch.cuda.synchronize()
+    if dist:
+        torch.distributed.barrier()
+    ms = t0.elapsed_time(t1) / steps
+    per = {nm: sum(ev[k][q].elapsed_time(ev[k][q + 1]) for k in range(steps)) / steps
+           for q, nm in enumerate(names)}
+    if dist:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms, per
+
+
+def roofline(step, per_ms, n, nodes, peak):
+    kb = step.kernel_bytes(n, nodes)
+    dom = max(per_ms, key=lambda k: per_ms[k])
+    ach = kb[dom] / (per_ms[dom] * 1e-3) / 1e9
+    kernels = {k: {"ms": per_ms[k], "bytes": kb[k],
+                   "gbs": kb[k] / (per_ms[k] * 1e-3) / 1e9 if per_ms[k] > 0 else None}
+               for k in per_ms}
+    return {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak["hbm_gbs"],
+            "unit": "GB/s", "frac": ach / peak["hbm_gbs"],
+            "peak_source": peak["source"], "traffic": None}, kernels
+
+
+def run_ours(args):
+    import torch
+
+    import picasso_b200 as pb
+    from picasso_b200 import workloads
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = world > 1
+    torch.cuda.set_device(local)
+    if dist:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    ORDER[0] = args.order
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+    n_cells = args.grid
+    mesh = pb.UniformMesh([0, 0, 0, 1, 1, 1], cell_size=1.0 / n_cells,
+                          periodic=(True, True, True))
+    seed = 1000 + (2 if args.workload == "clustered" else 1) + 17 * rank
+    x = workloads.positions(args.workload, n_cells, args.ppc, seed, device=dev)
+    n = x.shape[0]
+    nodes = n_cells ** 3
+    m64, c64 = workloads.particle_state(n, seed, device=dev)
+    sort_info = None
+    bins = None
+    if not args.unsorted:
+        sd0 = pb.create_spline(pb.FieldLocation.Node, args.order, mesh, x)
+        ws = None
+        for it in range(2):  # second run is timed
+            torch.cuda.synchronize()
+            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            e0.record()
+            key, perm, bins = pb.cell_sort(sd0, tuple(args.tile))
+            e1.record()
+            xs, ms_, cs = pb.permute_members(perm, x, m64, c64)
+            e2.record()
+            torch.cuda.synchronize()
+            sort_info = {"sort_ms": e0.elapsed_time(e1), "permute_ms": e1.elapsed_time(e2),
+                         "tile": list(args.tile), "num_tiles": bins.num_tiles}
+        x, m64, c64 = xs, ms_, cs
+        del key, perm, xs, ms_, cs
+    m32, c32 = m64.float(), c64.float()
+    peak = peaks()
+    clk = Clocks(local)
+
+    out = {}
+    # FP32 precision form (headline)
+    s32 = Step("fp32", mesh, x, m32, c32.clone(), bins, stream)
+    clk.start()
+    ms32, per32 = time_form(s32, args.steps, args.warmup, dist)
+    clocks = clk.stop()
+    rf32, k32 = roofline(s32, per32, n, nodes, peak)
+    out["fp32"] = (ms32, per32, rf32, k32)
+    # FP64 plain form
+    if not args.no_fp64:
+        s64 = Step("fp64", mesh, x, m64, c64.clone(), None, stream)
+        ms64, per64 = time_form(s64, args.steps, args.warmup, dist)
+        rf64, k64 = roofline(s64, per64, n, nodes, peak)
+        out["fp64"] = (ms64, per64, rf64, k64)
+        # per-field error of the FP32 form against the FP64 result of the
+        # same step (the FP64 form is parity-checked against the oracle)
+        s64.c.copy_(c64)
+        s32.c.copy_(c32)
+        s64.run()
+        s32.run()
+        torch.cuda.synchronize()
+        u64 = s64.u
+        u32 = s32.u.double()
+        den = u64.abs().max()
+        err = {"grid_velocity": float((u32 - u64).abs().max() / den),
+               "grid_mass": float((s32.gm.to_float() - s64.gm).abs().max() / s64.gm.abs().max()),
+               "grid_momentum": float((s32.gmu.to_float() - s64.gmu).abs().max()
+                                      / s64.gmu.abs().max()),
+               "particle_velocity": float((s32.c[:, 0].double() - s64.c[:, 0]).abs().max()
+                                          / s64.c[:, 0].abs().max()),
+               "particle_affine": float((s32.c[:, 1:].double() - s64.c[:, 1:]).abs().max()
+                                        / s64.c[:, 1:].abs().max())}
+        out["errors"] = err
+        del s64
+    # e2e through the C ABI with host buffers (FP32 form)
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(s32, x, m32, c32, args, stream, dist, world)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_sample(args, 3, 1, os.cpu_count() or 1)
+        cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+
+    ms32, per32, rf32, k32 = out["fp32"]
+    value = world * n / (ms32 * 1e-3)
+    model_bytes = 162.0
+    line = {"metric": METRIC, "value": value, "unit": "particles/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms32,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 (i64 fixed-point grid, f64 division/positions)", "data": "synthetic",
+            "config": config_of(args), "roofline": rf32,
+            "step_roofline": {"bytes_per_particle_model": model_bytes,
+                              "achieved_gbs": n * model_bytes / (ms32 * 1e-3) / 1e9,
+                              "frac": n * model_bytes / (ms32 * 1e-3) / 1e9 / peak["hbm_gbs"]},
+            "kernels": k32, "gpu_launches": s32.launches_per_step * args.steps,
+            "clocks": clocks}
+    if "fp64" in out:
+        ms64, per64, rf64, k64 = out["fp64"]
+        line["fp64_plain"] = {"value": world * n / (ms64 * 1e-3), "ms_per_step": ms64,
+                              "roofline": rf64, "kernels": k64,
+                              "step_frac": n * 262.0 / (ms64 * 1e-3) / 1e9 / peak["hbm_gbs"]}
+        line["speedup_fp32_vs_fp64"] = ms64 / ms32
+        line["errors_vs_fp64"] = out["errors"]
+    if sort_info:
+        line["sort"] = sort_info
+    if e2e:
+        line["e2e"] = e2e
+    if cpu:
+        line["cpu_baseline"] = cpu
+    if rank == 0:
+        print(json.dumps(line))
+        if args.json_out:
+            with open(args.json_out, "w") as f:
+                json.dump(line, f, indent=1)
+    if dist:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+def run_e2e(step, x, m32, c32, args, stream, dist, world):
+    """Same step with the particle arrays in pinned host memory: copy x, m, c
+    in, run, copy c (the step's result) out, every step."""
+    import torch
+    n = x.shape[0]
+    hx = torch.empty(x.shape, dtype=x.dtype, pin_memory=True)
+    hm = torch.empty(m32.shape, dtype=m32.dtype, pin_memory=True)
+    hc = torch.empty(c32.shape, dtype=c32.dtype, pin_memory=True)
+    hout = torch.empty(c32.shape, dtype=c32.dtype, pin_memory=True)
+    hx.copy_(x)
+    hm.copy_(m32)
+    hc.copy_(c32)
+    h2d = hx.numel() * 8 + hm.numel() * 4 + hc.numel() * 4
+    d2h = hout.numel() * 4
+    steps = max(1, min(args.steps, 3))
+
+    def one():
+        step.sd.x.copy_(hx, non_blocking=True)
+        step.m.copy_(hm, non_blocking=True)
+        step.c.copy_(hc, non_blocking=True)
+        step.run()
+        hout.copy_(step.c, non_blocking=True)
+
+    one()
+    torch.cuda.synchronize()
+    if dist:
+        torch.distributed.barrier()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(steps):
+        one()
+    t1.record(stream)
+    torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1) / steps
+    if dist:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    return {"value": world * n / (ms * 1e-3), "unit": "particles/s", "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h, "ms_per_step": ms, "steps": steps,
+            "path": "torch pinned copies + C-ABI transfer calls"}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

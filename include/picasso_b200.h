@@ -131,15 +131,21 @@ typedef struct picasso_grid_field {
 
 /* Particles sorted by stencil bin in tiles (output of picasso_cell_sort after
  * the particle arrays were permuted with picasso_permute).  With it the P2G
- * and G2P entry points use the shared-memory tiled kernels. */
+ * and G2P entry points use the shared-memory tiled kernels (FP32 precision
+ * form, collocated 3-component fields, packed storage: x_p (N,3) FP64,
+ * m_p (N) FP32, c_p (N,4,3) FP32 contiguous; other calls take the plain
+ * path).  Work items are chunks of at most `chunk` particles of one tile. */
 typedef struct picasso_bins {
-    int32_t tile[3];            /* bins per tile along i, j, k */
-    int32_t num_tiles[3];       /* tiles along i, j, k */
-    int32_t bin_extent[3];      /* bins along i, j, k */
-    int32_t order;              /* spline order the bins were built for */
-    int32_t location;           /* picasso_location the bins were built for */
-    int32_t pad_;
-    const int64_t* tile_offset; /* device, num_tiles_total + 1 particle offsets */
+    int32_t tile[3];             /* bins per tile along i, j, k */
+    int32_t num_tiles[3];        /* tiles along i, j, k */
+    int32_t bin_extent[3];       /* bins along i, j, k */
+    int32_t order;               /* spline order the bins were built for */
+    int32_t location;            /* picasso_location the bins were built for */
+    int32_t chunk;               /* particles per work item */
+    const int64_t* tile_offset;  /* device, num_tiles_total + 1 particle offsets */
+    const uint32_t* tile_items;  /* device, num_tiles_total + 1: first work item
+                                    of each tile (exclusive prefix of
+                                    ceil(count / chunk)) */
 } picasso_bins;
 
 /* Execution context of one call. */
@@ -264,12 +270,15 @@ PICASSO_API picasso_status picasso_cell_sort_workspace(const picasso_spline* sd,
  * (perm[r] = original index of the particle of rank r; ties keep the
  * original order) and tile_offset[num_tiles + 1] (first rank of each tile;
  * the last entry counts the particles inside the mesh).  bins_out (host) is
- * filled for picasso_exec.bins.  workspace: device memory of at least the
- * size picasso_cell_sort_workspace reports, 256-byte aligned.
+ * filled for picasso_exec.bins.  tile_items[num_tiles + 1] receives the
+ * work-item prefix for chunks of `chunk` particles (chunk >= 32).
+ * workspace: device memory of at least the size picasso_cell_sort_workspace
+ * reports, 256-byte aligned.
  * No reference counterpart: Picasso has no particle sort. */
 PICASSO_API picasso_status picasso_cell_sort(const picasso_spline* sd, int64_t num_particles,
                                  picasso_particle_field x_p, const int32_t tile[3],
-                                 uint32_t* key, uint32_t* perm, int64_t* tile_offset,
+                                 int32_t chunk, uint32_t* key, uint32_t* perm,
+                                 int64_t* tile_offset, uint32_t* tile_items,
                                  void* workspace, int64_t workspace_bytes,
                                  picasso_bins* bins_out, const picasso_exec* exec);
 

@@ -30,8 +30,8 @@ def build():
 def lib():
     global _lib
     if _lib is None:
-        if not os.path.exists(LIB):
-            build()
+        # make is a no-op when the library is up to date with its sources
+        build()
         L = C.CDLL(LIB)
         P = C.POINTER
         sig = {

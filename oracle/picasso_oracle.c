@@ -546,20 +546,19 @@ int oracle_polypic_g2p(const picasso_spline* sp, int64_t np, int ncomp,
                 G[d][1][n] = sd.g[d][n];
             }
         if (sp->order == 2) {
-            /* weighted least-squares projection onto the orthogonal modes:
-             * G = w s_deg(r) / sum_n w s_deg(r)^2 (the linear case reduces to
-             * w and dw/dx, PolyPIC.hpp:269-284) */
+            /* weighted least-squares projection onto the orthogonal modes,
+             * G = w s_deg(r) / sum_n w s_deg(r)^2.  With q = p / h the
+             * denominators are h^2/4 (degree 1) and h^4 (1-4q^2)^2 (3/4-q^2)/4
+             * (degree 2, the BTMB diagonal of polypic_2d_quadratic.nb), and
+             * the quotients simplify to G1 = 4 w r / h^2 and
+             * G2 = {1/(2h^2), -1/h^2, 1/(2h^2)}: the degree-2 quotient is a
+             * 0/0 limit at cell faces, so the closed forms are evaluated. */
             for (int d = 0; d < 3; ++d) {
-                double alpha = quad_alpha(&sd, d), h = sd.dx[d];
-                for (int deg = 1; deg < 3; ++deg) {
-                    double den = 0.0;
-                    for (int n = 0; n < nk; ++n) {
-                        double s = mode1d(deg, sd.d[d][n], h, alpha);
-                        den += sd.w[d][n] * s * s;
-                    }
-                    for (int n = 0; n < nk; ++n)
-                        G[d][deg][n] = sd.w[d][n] * mode1d(deg, sd.d[d][n], h, alpha) / den;
-                }
+                double h = sd.dx[d], rh2 = 1.0 / (h * h);
+                for (int n = 0; n < nk; ++n) G[d][1][n] = 4.0 * sd.w[d][n] * sd.d[d][n] * rh2;
+                G[d][2][0] = 0.5 * rh2;
+                G[d][2][1] = -rh2;
+                G[d][2][2] = 0.5 * rh2;
             }
         }
         double cp[27][3];
@@ -666,7 +665,7 @@ uint32_t oracle_particle_key(const picasso_spline* sp, const double xp[3], const
             if (r < 0) r += nb[d];
             b[d] = r;
         } else {
-            if (s < 0 || s + sd.nk > sp->mesh.extent[d]) return (uint32_t)nkeys;
+            if (s < 0 || s > sp->mesh.extent[d] - sd.nk) return (uint32_t)nkeys;
             b[d] = s;
         }
     }

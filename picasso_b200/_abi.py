@@ -57,7 +57,7 @@ class GridField(C.Structure):
 class Bins(C.Structure):
     _fields_ = [("tile", C.c_int32 * 3), ("num_tiles", C.c_int32 * 3),
                 ("bin_extent", C.c_int32 * 3), ("order", C.c_int32), ("location", C.c_int32),
-                ("pad_", C.c_int32), ("tile_offset", C.c_void_p)]
+                ("chunk", C.c_int32), ("tile_offset", C.c_void_p), ("tile_items", C.c_void_p)]
 
 
 class Exec(C.Structure):
@@ -92,8 +92,9 @@ SIGNATURES = [
     ("picasso_cell_sort_workspace", C.c_int,
      [C.POINTER(Spline), C.c_int64, C.POINTER(C.c_int32), C.POINTER(C.c_int64)]),
     ("picasso_cell_sort", C.c_int,
-     [C.POINTER(Spline), C.c_int64, ParticleField, C.POINTER(C.c_int32), C.c_void_p,
-      C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.POINTER(Bins), C.POINTER(Exec)]),
+     [C.POINTER(Spline), C.c_int64, ParticleField, C.POINTER(C.c_int32), C.c_int32, C.c_void_p,
+      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.POINTER(Bins),
+      C.POINTER(Exec)]),
     ("picasso_permute", C.c_int,
      [C.c_int64, C.c_int32, C.c_void_p, ParticleField, ParticleField, C.POINTER(Exec)]),
     ("picasso_mat3_inverse", C.c_int,

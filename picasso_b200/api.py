@@ -380,18 +380,21 @@ def advect(mesh_desc, x_p, c_p, dt, stream=None):
 class Bins:
     """Result of cell_sort: the C descriptor plus the tensors it points to."""
 
-    def __init__(self, desc, tile_offset):
+    def __init__(self, desc, tile_offset, tile_items):
         self.desc = desc
         self.tile_offset = tile_offset
+        self.tile_items = tile_items
 
     @property
     def num_tiles(self):
         return self.desc.num_tiles[0] * self.desc.num_tiles[1] * self.desc.num_tiles[2]
 
 
-def cell_sort(sd, tile=(8, 8, 8), stream=None, workspace=None):
+def cell_sort(sd, tile=(4, 8, 8), chunk=2048, stream=None, workspace=None):
     """Stable sort of the spline's particles by (tile, bin).  Returns
-    (key, perm, bins) as uint32-valued int32 / int64 CUDA tensors."""
+    (key, perm, bins): keys and permutation as int32 tensors holding uint32
+    values, and the Bins to pass to the transfers once the particle members
+    have been permuted (see permute / permute_members)."""
     lib = _lib()
     n = sd.num_particles
     t3 = (C.c_int32 * 3)(*tile)
@@ -409,12 +412,14 @@ def cell_sort(sd, tile=(8, 8, 8), stream=None, workspace=None):
         nb = m.own_extent[d] if m.periodic[d] else m.extent[d]
         nt *= -(-nb // tile[d])
     tile_offset = torch.empty(nt + 1, dtype=torch.int64, device=dev)
+    tile_items = torch.empty(nt + 1, dtype=torch.int32, device=dev)
     bins = _abi.Bins()
     ex = _exec(stream, None, None)
-    check(lib.picasso_cell_sort(C.byref(sd.desc), n, particle_field(sd.x), t3, key.data_ptr(),
-                                perm.data_ptr(), tile_offset.data_ptr(), workspace.data_ptr(),
-                                workspace.numel(), C.byref(bins), C.byref(ex.desc)), "cell_sort")
-    return key[:n], perm[:n], Bins(bins, tile_offset)
+    check(lib.picasso_cell_sort(C.byref(sd.desc), n, particle_field(sd.x), t3, int(chunk),
+                                key.data_ptr(), perm.data_ptr(), tile_offset.data_ptr(),
+                                tile_items.data_ptr(), workspace.data_ptr(), workspace.numel(),
+                                C.byref(bins), C.byref(ex.desc)), "cell_sort")
+    return key[:n], perm[:n], Bins(bins, tile_offset, tile_items)
 
 
 def permute(perm, src, dst=None, stream=None):

@@ -318,11 +318,15 @@ extern "C" picasso_status picasso_apic_p2g(const picasso_spline* sd, int64_t num
     PField x = make_pfield(x_p), m = make_pfield(m_p), c = make_pfield(c_p);
     GField gm = make_gfield(m_i), gmu = make_gfield(mu_i);
     if (exec && exec->bins) {
+        // bins describe particles sorted for this spline
+        if (exec->bins->order != sd->order || exec->bins->location != sd->location)
+            return PICASSO_ERR_INVALID_ARGUMENT;
         bool handled = false;
-        st = apic_p2g_tiled(mp, sd->order, ncomp, form, num_particles, x, m, c, gm, gmu,
-                            *exec->bins, err, s, &handled);
-        if (st || handled) return st;
-        if (exec->bins->order != sd->order) return PICASSO_ERR_INVALID_ARGUMENT;
+        if (stag < 0) {
+            st = apic_p2g_tiled(mp, sd->order, ncomp, form, num_particles, x, m, c, gm, gmu,
+                                *exec->bins, err, s, &handled);
+            if (st || handled) return st;
+        }
     }
     return apic_p2g_plain(mp, sd->order, stag, ncomp, form, num_particles, x, m, c, gm, gmu,
                           err, s);
@@ -349,10 +353,14 @@ extern "C" picasso_status picasso_apic_g2p(const picasso_spline* sd, int64_t num
     PField x = make_pfield(x_p), c = make_pfield(c_p);
     GField u = make_gfield(u_i);
     if (exec && exec->bins) {
+        if (exec->bins->order != sd->order || exec->bins->location != sd->location)
+            return PICASSO_ERR_INVALID_ARGUMENT;
         bool handled = false;
-        st = apic_g2p_tiled(mp, sd->order, ncomp, f32, num_particles, x, u, c, *exec->bins, err,
-                            s, &handled);
-        if (st || handled) return st;
+        if (stag < 0) {
+            st = apic_g2p_tiled(mp, sd->order, ncomp, f32, num_particles, x, u, c, *exec->bins,
+                                err, s, &handled);
+            if (st || handled) return st;
+        }
     }
     return apic_g2p_plain(mp, sd->order, stag, ncomp, f32, num_particles, x, u, c, err, s);
 }

@@ -290,7 +290,8 @@ __device__ __forceinline__ bool resolve_stencil(const MeshP& mp, int d, int s0, 
         }
         return true;
     }
-    if (s0 < 0 || s0 + K > mp.ext[d]) return false;
+    // written so that no sum can overflow for non-finite positions
+    if (s0 < 0 || s0 > mp.ext[d] - K) return false;
 #pragma unroll
     for (int q = 0; q < K; ++q) idx[q] = s0 + q;
     return true;

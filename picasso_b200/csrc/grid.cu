@@ -104,7 +104,8 @@ __global__ void advect_kernel(int64_t n, PField x, PField c, double dt, int3 per
         const double ln[3] = {len.x, len.y, len.z};
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-            double xn = x.get<double>(p, d) + dt * (double)c.get<CT>(p, d);
+            // rounded step by step, as the FP64 update x + (dt * v)
+            double xn = __dadd_rn(x.get<double>(p, d), __dmul_rn(dt, (double)c.get<CT>(p, d)));
             if (per[d]) {
                 if (xn < l0[d]) xn += ln[d];
                 else if (xn >= l0[d] + ln[d]) xn -= ln[d];

@@ -190,20 +190,16 @@ polypic_g2p_kernel(MeshP mp, int64_t n, PField x, GField u, PField c, int col, i
                 G[d][2][q] = R(0);
             }
             if (ORDER == 2) {
+                // closed forms of w s_g(r) / sum_n w s_g(r)^2: G1 = 4 w r / h^2,
+                // G2 = {1/(2h^2), -1/h^2, 1/(2h^2)} (the degree-2 quotient is
+                // a 0/0 limit at cell faces)
                 const R h = (R)mp.dx[d];
-                const R alpha = quad_alpha(-sp[d].d[1], h);
+                const R rh2 = R(1) / (h * h);
 #pragma unroll
-                for (int g = 1; g < 3; ++g) {
-                    R den = R(0);
-#pragma unroll
-                    for (int q = 0; q < K; ++q) {
-                        const R s = mode1d(g, sp[d].d[q], h, alpha);
-                        den += sp[d].w[q] * s * s;
-                    }
-#pragma unroll
-                    for (int q = 0; q < K; ++q)
-                        G[d][g][q] = sp[d].w[q] * mode1d(g, sp[d].d[q], h, alpha) / den;
-                }
+                for (int q = 0; q < K; ++q) G[d][1][q] = R(4) * sp[d].w[q] * sp[d].d[q] * rh2;
+                G[d][2][0] = R(0.5) * rh2;
+                G[d][2][1] = -rh2;
+                G[d][2][2] = R(0.5) * rh2;
             }
         }
         R cp[NM][NCU];

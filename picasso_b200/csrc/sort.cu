@@ -49,7 +49,7 @@ __device__ __forceinline__ uint32_t particle_key(const BinP& bp, const double xs
             if (r < 0) r += bp.nb[d];
             b[d] = r;
         } else {
-            if (s < 0 || s + K > bp.mp.ext[d]) return bp.nkeys;
+            if (s < 0 || s > bp.mp.ext[d] - K) return bp.nkeys;
             b[d] = s;
         }
     }
@@ -258,6 +258,16 @@ __global__ void tile_offset_kernel(const uint32_t* __restrict__ keys, int64_t n,
     }
 }
 
+__global__ void tile_items_kernel(const int64_t* __restrict__ tile_offset, int64_t ntiles,
+                                  int chunk, uint32_t* __restrict__ items)
+{
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t <= ntiles;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t cnt = t < ntiles ? tile_offset[t + 1] - tile_offset[t] : 0;
+        items[t] = (uint32_t)((cnt + chunk - 1) / chunk);
+    }
+}
+
 template <class T>
 __global__ void permute_kernel(int64_t n, int ncomp, const uint32_t* __restrict__ perm, PField src,
                                PField dst)
@@ -310,7 +320,9 @@ static picasso_status make_plan(const picasso_spline* sd, int64_t n, const int32
     pl->width = (bits + pl->passes - 1) / pl->passes;
     pl->nblk = (n + kSortTile - 1) / kSortTile;
     if (pl->nblk < 1) pl->nblk = 1;
+    // the digit table is also reused for the per-tile work-item counts
     pl->hist_len = (int64_t(1) << pl->width) * pl->nblk;
+    if (pl->hist_len < pl->ntiles + 1) pl->hist_len = pl->ntiles + 1;
     pl->scan_blocks = (pl->hist_len + kScanTile - 1) / kScanTile;
     int64_t o = 0;
     pl->off_keys = o;
@@ -345,7 +357,8 @@ extern "C" picasso_status picasso_cell_sort_workspace(const picasso_spline* sd,
 
 extern "C" picasso_status picasso_cell_sort(const picasso_spline* sd, int64_t num_particles,
                                             picasso_particle_field x_p, const int32_t tile[3],
-                                            uint32_t* key, uint32_t* perm, int64_t* tile_offset,
+                                            int32_t chunk, uint32_t* key, uint32_t* perm,
+                                            int64_t* tile_offset, uint32_t* tile_items,
                                             void* workspace, int64_t workspace_bytes,
                                             picasso_bins* bins_out, const picasso_exec* exec)
 {
@@ -353,7 +366,8 @@ extern "C" picasso_status picasso_cell_sort(const picasso_spline* sd, int64_t nu
     picasso_status st = make_plan(sd, num_particles, tile, &pl);
     if (st) return st;
     if ((st = validate_pfield(x_p, PICASSO_F64))) return st;
-    if (!key || !perm || !tile_offset || !workspace || workspace_bytes < pl.bytes)
+    if (!key || !perm || !tile_offset || !tile_items || !workspace ||
+        workspace_bytes < pl.bytes || chunk < 32)
         return PICASSO_ERR_INVALID_ARGUMENT;
     if (reinterpret_cast<uintptr_t>(workspace) % 256) return PICASSO_ERR_INVALID_ARGUMENT;
     const int64_t n = num_particles;
@@ -396,6 +410,15 @@ extern "C" picasso_status picasso_cell_sort(const picasso_spline* sd, int64_t nu
     }
     tile_offset_kernel<<<grid_for(pl.ntiles + 1, 256), 256, 0, s>>>(key, n, pl.ntiles, pl.bp.tsize,
                                                                      tile_offset);
+    // work items: exclusive prefix of ceil(count / chunk) per tile
+    {
+        const int64_t m = pl.ntiles + 1;
+        const int64_t sb = (m + kScanTile - 1) / kScanTile;
+        tile_items_kernel<<<grid_for(m, 256), 256, 0, s>>>(tile_offset, pl.ntiles, chunk, hist);
+        scan_reduce_kernel<<<(unsigned)sb, kScanThreads, 0, s>>>(hist, m, sums);
+        scan_sums_kernel<<<1, kScanThreads, 0, s>>>(sums, sb);
+        scan_apply_kernel<<<(unsigned)sb, kScanThreads, 0, s>>>(hist, tile_items, m, sums);
+    }
     if ((st = check_launch())) return st;
     if (bins_out) {
         for (int d = 0; d < 3; ++d) {
@@ -405,8 +428,9 @@ extern "C" picasso_status picasso_cell_sort(const picasso_spline* sd, int64_t nu
         }
         bins_out->order = sd->order;
         bins_out->location = sd->location;
-        bins_out->pad_ = 0;
+        bins_out->chunk = chunk;
         bins_out->tile_offset = tile_offset;
+        bins_out->tile_items = tile_items;
     }
     return PICASSO_OK;
 }

@@ -1,0 +1,119 @@
+"""Cell sort (bit-exact permutation vs the oracle's stable counting sort),
+permutation gather, grid velocity update, advection and batched 3x3
+inverse on the GPU through the C ABI."""
+
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from particles import clustered_particles, periodic_mesh, rel_err, uniform_particles
+from picasso_b200 import (FieldLocation, UniformMesh, advect, cell_sort, create_spline,
+                          grid_velocity, mat3_inverse, permute)
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev(a, dtype=torch.float64):
+    return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype, device="cuda")
+
+
+@pytest.mark.parametrize("order", [1, 2, 3])
+@pytest.mark.parametrize("tile", [(4, 4, 4), (8, 4, 2), (1, 1, 1)])
+def test_cell_sort_matches_oracle(cuda, order, tile):
+    mesh = periodic_mesh(16, halo=1)
+    x, _, _ = clustered_particles(mesh, 16 ** 3 * 6, nblob=3, sigma_cells=1.5, frac=0.6,
+                                  seed=order)
+    sdo = create_spline(FieldLocation.Node, order, mesh, None).desc
+    key_o, perm_o, off_o = oracle.cell_sort(sdo, x, tile)
+    sd = create_spline(FieldLocation.Node, order, mesh, _dev(x))
+    key, perm, bins = cell_sort(sd, tile)
+    assert np.array_equal(key.cpu().numpy().view(np.uint32), key_o)
+    assert np.array_equal(perm.cpu().numpy().view(np.uint32), perm_o)
+    assert np.array_equal(bins.tile_offset.cpu().numpy(), off_o)
+
+
+def test_cell_sort_non_periodic_out_of_mesh_last(cuda):
+    mesh = UniformMesh([0, 0, 0, 1, 1, 1], cell_size=1 / 8, periodic=(False, False, False),
+                       halo_cell_width=1)
+    rng = np.random.default_rng(5)
+    x = rng.uniform(-0.3, 1.3, (5000, 3))
+    sdo = create_spline(FieldLocation.Cell, 2, mesh, None).desc
+    key_o, perm_o, off_o = oracle.cell_sort(sdo, x, (4, 4, 4))
+    key, perm, bins = cell_sort(create_spline(FieldLocation.Cell, 2, mesh, _dev(x)), (4, 4, 4))
+    assert np.array_equal(perm.cpu().numpy().view(np.uint32), perm_o)
+    assert np.array_equal(bins.tile_offset.cpu().numpy(), off_o)
+    assert off_o[-1] < x.shape[0]  # some particles are outside and sort last
+
+
+def test_cell_sort_large_is_stable_and_sorted(cuda):
+    """Size-independent properties at a larger size: keys ascending, the
+    permutation is a bijection and ties keep the original order."""
+    mesh = periodic_mesh(64, halo=0)
+    x, _, _ = clustered_particles(mesh, 64 ** 3 * 8, nblob=32, sigma_cells=2.0, frac=0.7, seed=9)
+    sd = create_spline(FieldLocation.Node, 2, mesh, _dev(x))
+    key, perm, bins = cell_sort(sd, (8, 8, 8))
+    k = key.to(torch.int64) & 0xFFFFFFFF
+    p = perm.to(torch.int64) & 0xFFFFFFFF
+    assert bool((k[1:] >= k[:-1]).all())
+    same = k[1:] == k[:-1]
+    assert bool((p[1:][same] > p[:-1][same]).all())
+    assert torch.equal(torch.sort(p).values, torch.arange(x.shape[0], device="cuda"))
+
+
+def test_permute(cuda):
+    rng = np.random.default_rng(2)
+    src = _dev(rng.standard_normal((1000, 4, 3)))
+    perm = torch.as_tensor(rng.permutation(1000).astype(np.int32), device="cuda")
+    dst = permute(perm, src)
+    assert torch.equal(dst, src[perm.long()])
+    s32 = src.float()
+    assert torch.equal(permute(perm, s32), s32[perm.long()])
+
+
+def test_grid_velocity_vs_oracle(cuda):
+    mesh = periodic_mesh(12, halo=1)
+    ext = mesh.extent(FieldLocation.Node)
+    rng = np.random.default_rng(4)
+    gm = rng.uniform(0, 2, ext)
+    gm[rng.random(ext) < 0.2] = 0.0
+    gmu = rng.standard_normal(ext + (3,))
+    desc = mesh.descriptor(FieldLocation.Node)
+    gu_o = np.zeros_like(gmu)
+    oracle.grid_velocity(desc, gm, gmu, gu_o, 1e-12)
+    gu = torch.zeros(ext + (3,), dtype=torch.float64, device="cuda")
+    grid_velocity(desc, _dev(gm), _dev(gmu), gu, 1e-12)
+    assert np.array_equal(gu.cpu().numpy(), gu_o)
+
+
+def test_advect_vs_oracle(cuda):
+    mesh = periodic_mesh(8, halo=0)
+    x, _, c = uniform_particles(mesh, 2, seed=6)
+    c[:, 0] *= 5.0
+    desc = mesh.descriptor(FieldLocation.Node)
+    xo = x.copy()
+    v = np.ascontiguousarray(c[:, 0])
+    oracle.advect(desc, xo, v, 0.02)
+    xd = _dev(x)
+    advect(desc, xd, _dev(c), 0.02)
+    got = xd.cpu().numpy()
+    assert np.array_equal(got, xo)
+    assert got.min() >= 0.0 and got.max() < 1.0
+
+
+def test_mat3_inverse(cuda):
+    rng = np.random.default_rng(3923423)
+    n = 1000
+    a = rng.uniform(-1, 1, (n, 3, 3))
+    x0 = rng.uniform(-1, 1, (n, 3))
+    # the reference's kernel test builds op = 0.75 (A + 0.5 A^T) and solves
+    # op x1 = op x0 (tstBatchedLinearAlgebra.hpp:1769-1789); here with the
+    # cofactor inverse, same tolerance 1e-11
+    op = 0.75 * (a + 0.5 * np.transpose(a, (0, 2, 1)))
+    b = np.einsum("nij,nj->ni", op, x0)
+    inv, det, y = mat3_inverse(_dev(op), _dev(b))
+    inv_o, det_o, y_o = oracle.mat3_inverse(op, b)
+    assert rel_err(det.cpu().numpy(), det_o) <= 1e-14
+    assert rel_err(inv.cpu().numpy(), inv_o) <= 1e-12
+    cond_ok = np.abs(det_o) > 1e-3
+    np.testing.assert_allclose(y.cpu().numpy()[cond_ok], x0[cond_ok], rtol=0, atol=1e-11)
