@@ -270,8 +270,7 @@ __device__ __forceinline__ void spline_eval_frac(double x, double lo, double dx,
     // particle at t - shift
 #pragma unroll
     for (int n = 0; n < SplineTraits<ORDER>::K; ++n)
-        sp.d[n] = (R)((double)(SplineTraits<ORDER>::first + n) + SplineTraits<ORDER>::shift -
-                      (double)t) * h;
+        sp.d[n] = (R(SplineTraits<ORDER>::first + n + SplineTraits<ORDER>::shift) - t) * h;
 }
 
 // Periodic wrap / bounds check of a stencil start: fills the K resolved

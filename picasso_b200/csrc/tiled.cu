@@ -5,7 +5,7 @@
 // Work items are chunks of at most `chunk` particles of one tile (the sort
 // writes the per-tile item prefix).
 //
-// P2G (one warp per item): every lane sweeps its own contiguous run of the
+// P2G (one single-warp CTA per item): every lane sweeps its own contiguous run of the
 // item's particles -- sorted by bin, so consecutive particles mostly share a
 // stencil -- and accumulates the 4 x K^3 mass / momentum contributions of its
 // current bin in registers.  Particle records arrive through a per-lane
@@ -40,6 +40,9 @@ struct TileP {
     int nb[3];   // bins per dimension
     int NT[3];   // nodes per tile dimension (T + K - 1)
     int nodes;   // NT0 * NT1 * NT2
+    int SJ, SI;  // P2G node-tile strides along j and i (k stride 1), padded so
+    int P;       // the 27 (64) stencil nodes of a merge hit distinct banks;
+                 // P = stride between the 4 field planes
     int chunk;
     int64_t ntiles;
     const int64_t* off;     // tile particle offsets (ntiles + 1)
@@ -49,8 +52,14 @@ struct TileP {
 __device__ __forceinline__ int bin_of(const MeshP& mp, const TileP& tp, int d, int s0)
 {
     if (mp.periodic[d]) {
-        int r = (s0 - mp.own_lo[d]) % tp.nb[d];
-        if (r < 0) r += tp.nb[d];
+        const int nb = tp.nb[d];
+        int r = s0 - mp.own_lo[d];
+        if (r < 0) r += nb;          // one period covers every particle inside or
+        else if (r >= nb) r -= nb;   // next to the owned box
+        if ((unsigned)r >= (unsigned)nb) {
+            r %= nb;
+            if (r < 0) r += nb;
+        }
         return r;
     }
     return s0;
@@ -240,7 +249,7 @@ struct MergePlan {
             moff[r] = 0;
             if (v < 4 * A::FS && nn < A::KKK) {
                 const int a = nn / (K * K), b = (nn / K) % K, c = nn % K;
-                moff[r] = f * tp.nodes + (a * tp.NT[1] + b) * tp.NT[2] + c;
+                moff[r] = f * tp.P + a * tp.SI + b * tp.SJ + c;
                 valid |= 1u << r;
             }
         }
@@ -255,10 +264,12 @@ __device__ __forceinline__ void merge_partials(unsigned mask, P2GAcc<ORDER>& acc
                                                float* stage, int* stage_base, int lane)
 {
     while (mask) {
-        unsigned batch = 0, mm = mask;
+        unsigned batch = mask;
+        if (__popc(mask) > kStageLanes) {  // lowest kStageLanes lanes
+            batch = 0;
+            unsigned mm = mask;
 #pragma unroll
-        for (int q = 0; q < kStageLanes; ++q) {
-            if (mm) {
+            for (int q = 0; q < kStageLanes; ++q) {
                 batch |= mm & (~mm + 1u);
                 mm &= mm - 1u;
             }
@@ -284,35 +295,34 @@ __device__ __forceinline__ void merge_partials(unsigned mask, P2GAcc<ORDER>& acc
 }
 
 template <int ORDER>
-__global__ void __launch_bounds__(kWarps * 32, 2)
+__global__ void __launch_bounds__(32, 8)
 p2g_tiled_kernel(MeshP mp, TileP tp, int64_t n, const double* __restrict__ xg,
                  const float* __restrict__ mg, const float* __restrict__ cg, GField gm, GField gmu,
                  float scale_m, float scale_mu, int* err)
 {
     using A = P2GAcc<ORDER>;
     constexpr int K = A::K;
+    // one warp per CTA: warps finish their items independently
     extern __shared__ __align__(16) float smem[];
-    __shared__ int stage_base_all[kWarps][kStageLanes];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int per_warp = kRing * 32 * kSlot + kStageLanes * kStageStride + 4 * tp.nodes;
-    float* ring = smem + (size_t)warp * per_warp;
+    __shared__ int stage_base[kStageLanes];
+    const int lane = threadIdx.x;
+    float* ring = smem;
     float* stage = ring + kRing * 32 * kSlot;
     float* tile = stage + kStageLanes * kStageStride;
-    int* stage_base = stage_base_all[warp];
 
     if (blockIdx.x == 0 && threadIdx.x == 0 && err) {
         const int64_t n_valid = __ldg(tp.off + tp.ntiles);
         if (n > n_valid) atomicAdd(err, (int)(n - n_valid));
     }
     int64_t t, a, b;
-    if (!item_range(tp, (int64_t)blockIdx.x * kWarps + warp, t, a, b)) return;  // warp-uniform
+    if (!item_range(tp, blockIdx.x, t, a, b)) return;
     int ob[3];
     tile_origin(tp, t, ob);
     const int U = (int)((b - a + 31) / 32);
     const int64_t my0 = a + (int64_t)lane * U;
     const int cnt = (int)max((int64_t)0, min(my0 + U, b) - my0);
 
-    for (int i = lane; i < 4 * tp.nodes; i += 32) tile[i] = 0.f;
+    for (int i = lane; i < 4 * tp.P; i += 32) tile[i] = 0.f;
     MergePlan<ORDER> plan;
     plan.init(tp, lane);
     const float D = (ORDER >= 2) ? inertial_scaling<ORDER, float>(mp.dx[0]) : 0.f;
@@ -341,6 +351,7 @@ p2g_tiled_kernel(MeshP mp, TileP tp, int64_t n, const double* __restrict__ xg,
     int cur = -1, cur_base = 0;
     int bmin[3] = {1 << 30, 1 << 30, 1 << 30}, bmax[3] = {-1, -1, -1};
     for (int s = 0; s < U; ++s) {
+        __syncwarp();  // no lane still reads the slot refilled next
         issue(s + kRing - 1);
         cp_async_wait<kRing - 1>();
         const bool valid = s < cnt;
@@ -370,7 +381,7 @@ p2g_tiled_kernel(MeshP mp, TileP tp, int64_t n, const double* __restrict__ xg,
         if (ok) {
             if (lbin != cur) {
                 cur = lbin;
-                cur_base = (lb[0] * tp.NT[1] + lb[1]) * tp.NT[2] + lb[2];
+                cur_base = lb[0] * tp.SI + lb[1] * tp.SJ + lb[2];
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
                     bmin[d] = min(bmin[d], lb[d]);
@@ -399,13 +410,13 @@ p2g_tiled_kernel(MeshP mp, TileP tp, int64_t n, const double* __restrict__ xg,
         const int k = bmin[2] + e % e2;
         const int j = bmin[1] + (e / e2) % e1;
         const int i = bmin[0] + e / (e1 * e2);
-        const int idx = (i * tp.NT[1] + j) * tp.NT[2] + k;
+        const int idx = i * tp.SI + j * tp.SJ + k;
         const int gi = node_global(mp, tp, 0, ob[0], i);
         const int gj = node_global(mp, tp, 1, ob[1], j);
         const int gk = node_global(mp, tp, 2, ob[2], k);
 #pragma unroll
         for (int f = 0; f < 4; ++f) {
-            const float v = tile[f * tp.nodes + idx];
+            const float v = tile[f * tp.P + idx];
             if (v != 0.f) {
                 const long long q = __float2ll_rn(v * (f == 0 ? scale_m : scale_mu));
                 unsigned long long* dst = reinterpret_cast<unsigned long long*>(
@@ -483,29 +494,48 @@ g2p_tiled_kernel(MeshP mp, TileP tp, int64_t n, const double* __restrict__ xg, G
             continue;
         }
         const int base = (lb[0] * tp.NT[1] + lb[1]) * tp.NT[2] + lb[2];
+        // APIC.hpp:439-461, contracted one dimension at a time:
+        //   u_p    = sum_i wx_i sum_j wy_j sum_k wz_k u_ijk
+        //   B_p(:,q) = sum_ijk w_ijk u_ijk dist_q  (dist_q along x, y or z)
         float up[3] = {0.f, 0.f, 0.f};
         float B[3][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
-        // APIC.hpp:439-461
+        float wzdz[K];
 #pragma unroll
-        for (int i = 0; i < K; ++i)
+        for (int k = 0; k < K; ++k) wzdz[k] = sp[2].w[k] * sp[2].d[k];
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            float A0[3] = {0.f, 0.f, 0.f}, A1[3] = {0.f, 0.f, 0.f}, A2[3] = {0.f, 0.f, 0.f};
 #pragma unroll
             for (int j = 0; j < K; ++j) {
-                const float wij = sp[0].w[i] * sp[1].w[j];
                 const float4* row = tile + base + (i * tp.NT[1] + j) * tp.NT[2];
+                float S0[3] = {0.f, 0.f, 0.f}, S1[3] = {0.f, 0.f, 0.f};
 #pragma unroll
                 for (int k = 0; k < K; ++k) {
-                    const float w = wij * sp[2].w[k];
                     const float4 ue = row[k];
-                    const float wu[3] = {w * ue.x, w * ue.y, w * ue.z};
-                    const float dist[3] = {sp[0].d[i], sp[1].d[j], sp[2].d[k]};
+                    const float uk[3] = {ue.x, ue.y, ue.z};
 #pragma unroll
                     for (int d = 0; d < 3; ++d) {
-                        up[d] += wu[d];
-#pragma unroll
-                        for (int q = 0; q < 3; ++q) B[d][q] += wu[d] * dist[q];
+                        S0[d] += sp[2].w[k] * uk[d];
+                        S1[d] += wzdz[k] * uk[d];
                     }
                 }
+                const float wy = sp[1].w[j], wydy = wy * sp[1].d[j];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    A0[d] += wy * S0[d];
+                    A1[d] += wydy * S0[d];
+                    A2[d] += wy * S1[d];
+                }
             }
+            const float wx = sp[0].w[i], wxdx = wx * sp[0].d[i];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                up[d] += wx * A0[d];
+                B[d][0] += wxdx * A0[d];
+                B[d][1] += wx * A1[d];
+                B[d][2] += wx * A2[d];
+            }
+        }
         // c_p(0, d) = u_p(d); c_p(1 + q, d) = B_p(d, q)  (APIC.hpp:464-471)
         float4* out = reinterpret_cast<float4*>(cg + 12 * p);
         out[0] = make_float4(up[0], up[1], up[2], B[0][0]);
@@ -517,6 +547,61 @@ g2p_tiled_kernel(MeshP mp, TileP tp, int64_t n, const double* __restrict__ xg, G
 // ---------------------------------------------------------------------------
 // host dispatch
 // ---------------------------------------------------------------------------
+// Padded node-tile strides for the P2G merge: value v = lane + 32 r of a
+// staged lane (field v / FS, stencil node v % FS) lands at
+// f * P + a * SI + b * SJ + c; pick the smallest padding that maximises the
+// number of distinct banks per merge instruction.  Cached per tile shape.
+static void choose_strides(const int NT[3], int K, int* SJ, int* SI, int* P)
+{
+    static thread_local int cache_key[5] = {-1, -1, -1, -1, -1};
+    static thread_local int cache_val[3];
+    if (cache_key[0] == NT[0] && cache_key[1] == NT[1] && cache_key[2] == NT[2] &&
+        cache_key[3] == K) {
+        *SJ = cache_val[0];
+        *SI = cache_val[1];
+        *P = cache_val[2];
+        return;
+    }
+    const int KKK = K * K * K, FS = (KKK + 3) & ~3;
+    int best = -1, bsj = NT[2], bsi = NT[1] * NT[2], bp = NT[0] * NT[1] * NT[2];
+    long best_size = 0;
+    for (int sj = NT[2]; sj < NT[2] + 8; ++sj)
+        for (int si = NT[1] * sj; si < NT[1] * sj + 16; ++si)
+            for (int pp = NT[0] * si; pp < NT[0] * si + 16; ++pp) {
+                int distinct = 0;
+                for (int r = 0; r < 4; ++r) {
+                    unsigned banks = 0;
+                    for (int lane = 0; lane < 32; ++lane) {
+                        const int v = lane + 32 * r, f = v / FS, nn = v % FS;
+                        if (v >= 4 * FS || nn >= KKK) continue;
+                        const int a = nn / (K * K), b = (nn / K) % K, c = nn % K;
+                        const int off = f * pp + a * si + b * sj + c;
+                        const unsigned bit = 1u << (off & 31);
+                        if (!(banks & bit)) ++distinct;
+                        banks |= bit;
+                    }
+                }
+                const long size = 4L * pp;
+                if (distinct > best || (distinct == best && size < best_size)) {
+                    best = distinct;
+                    best_size = size;
+                    bsj = sj;
+                    bsi = si;
+                    bp = pp;
+                }
+            }
+    *SJ = bsj;
+    *SI = bsi;
+    *P = bp;
+    cache_key[0] = NT[0];
+    cache_key[1] = NT[1];
+    cache_key[2] = NT[2];
+    cache_key[3] = K;
+    cache_val[0] = bsj;
+    cache_val[1] = bsi;
+    cache_val[2] = bp;
+}
+
 static bool make_tilep(const MeshP& mp, int order, const picasso_bins& bins, TileP* tp)
 {
     const int K = order + 1;
@@ -532,6 +617,7 @@ static bool make_tilep(const MeshP& mp, int order, const picasso_bins& bins, Til
         nt *= bins.num_tiles[d];
     }
     tp->nodes = tp->NT[0] * tp->NT[1] * tp->NT[2];
+    choose_strides(tp->NT, K, &tp->SJ, &tp->SI, &tp->P);
     tp->ntiles = nt;
     tp->off = bins.tile_offset;
     tp->items = bins.tile_items;
@@ -572,8 +658,8 @@ static int64_t item_bound(const TileP& tp, int64_t n)
 template <int ORDER>
 static size_t p2g_smem(const TileP& tp)
 {
-    return sizeof(float) * (size_t)kWarps *
-           ((size_t)kRing * 32 * kSlot + kStageLanes * kStageStride + 4 * (size_t)tp.nodes);
+    return sizeof(float) *
+           ((size_t)kRing * 32 * kSlot + kStageLanes * kStageStride + 4 * (size_t)tp.P);
 }
 
 template <int ORDER>
@@ -586,8 +672,7 @@ static picasso_status launch_p2g_tiled(const MeshP& mp, const TileP& tp, int64_t
     PB_CUDA_TRY(cudaFuncSetAttribute(p2g_tiled_kernel<ORDER>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int64_t items = item_bound(tp, n);
-    const unsigned blocks = (unsigned)((items + kWarps - 1) / kWarps);
-    p2g_tiled_kernel<ORDER><<<blocks ? blocks : 1, kWarps * 32, smem, st>>>(
+    p2g_tiled_kernel<ORDER><<<(unsigned)(items ? items : 1), 32, smem, st>>>(
         mp, tp, n, reinterpret_cast<const double*>(x.data), reinterpret_cast<const float*>(m.data),
         reinterpret_cast<const float*>(c.data), gm, gmu, ldexpf(1.f, gm.fixed_bits),
         ldexpf(1.f, gmu.fixed_bits), err);
