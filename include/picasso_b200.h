@@ -282,6 +282,29 @@ PICASSO_API picasso_status picasso_cell_sort(const picasso_spline* sd, int64_t n
                                  void* workspace, int64_t workspace_bytes,
                                  picasso_bins* bins_out, const picasso_exec* exec);
 
+/* picasso_cell_sort for callers that cannot allocate device memory when they
+ * sort (an application that gives all GPU memory to its own pool at start-up,
+ * a plugin hosted by one, a loop that must not meet the allocator's latency
+ * or out-of-memory path).  Same arguments and results as picasso_cell_sort
+ * minus the workspace: the scratch is a 32 MiB array compiled into the
+ * library, held by every device that loads the library's kernels until the
+ * process exits.  Returns PICASSO_ERR_OUT_OF_RANGE, before any launch, when
+ * the sort needs more than 32 MiB (picasso_cell_sort_workspace reports the
+ * need; about 8 bytes per particle plus the digit tables, i.e. up to roughly
+ * 3 million particles).  The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress); make that first call before any
+ * stream capture.  All calls share the array: calls whose work overlaps on the
+ * GPU (other streams, other host threads) race, so order them.  No
+ * counterpart in the reference. */
+PICASSO_API picasso_status picasso_cell_sort_static(const picasso_spline* sd,
+                                                    int64_t num_particles,
+                                                    picasso_particle_field x_p,
+                                                    const int32_t tile[3], int32_t chunk,
+                                                    uint32_t* key, uint32_t* perm,
+                                                    int64_t* tile_offset, uint32_t* tile_items,
+                                                    picasso_bins* bins_out,
+                                                    const picasso_exec* exec);
+
 /* Gather a particle member: dst(p, c) = src(perm[p], c) for c < ncomp.
  * src and dst must not overlap. */
 PICASSO_API picasso_status picasso_permute(int64_t num_particles, int32_t ncomp, const uint32_t* perm,

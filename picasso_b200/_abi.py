@@ -95,6 +95,9 @@ SIGNATURES = [
      [C.POINTER(Spline), C.c_int64, ParticleField, C.POINTER(C.c_int32), C.c_int32, C.c_void_p,
       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.POINTER(Bins),
       C.POINTER(Exec)]),
+    ("picasso_cell_sort_static", C.c_int,
+     [C.POINTER(Spline), C.c_int64, ParticleField, C.POINTER(C.c_int32), C.c_int32, C.c_void_p,
+      C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(Bins), C.POINTER(Exec)]),
     ("picasso_permute", C.c_int,
      [C.c_int64, C.c_int32, C.c_void_p, ParticleField, ParticleField, C.POINTER(Exec)]),
     ("picasso_mat3_inverse", C.c_int,

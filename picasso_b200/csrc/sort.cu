@@ -10,6 +10,7 @@
 // original order (warp __match_any_sync + a per-warp running count, then a
 // prefix over the block's warps), so every pass is stable.
 #include <cmath>
+#include <mutex>
 
 #include "common.cuh"
 
@@ -454,4 +455,62 @@ extern "C" picasso_status picasso_permute(int64_t num_particles, int32_t ncomp,
         permute_kernel<float><<<blocks, 256, 0, s>>>(num_particles, ncomp, perm, make_pfield(src),
                                                      make_pfield(dst));
     return check_launch();
+}
+
+// ---------------------------------------------------------------------------
+// Cell sort without allocation
+// ---------------------------------------------------------------------------
+// Callers that cannot allocate device memory when they sort -- an application
+// that hands all of the GPU's memory to its own pool at start-up, a plugin
+// hosted by such an application, or a time-critical loop that must never hit
+// the allocator's latency or out-of-memory path -- get a sort whose scratch
+// is a fixed array compiled into this library.  The array is
+// kStaticSortScratchBytes large; every device on which the library's kernels
+// are loaded holds it until the process exits.
+namespace pb {
+
+constexpr int64_t kStaticSortScratchBytes = 32LL << 20;  // 32 MiB
+static __device__ __align__(256) unsigned char g_sort_scratch[kStaticSortScratchBytes];
+
+// Device address of g_sort_scratch on the current device, looked up once per
+// device (the host-side name of a __device__ array is not a device address).
+static picasso_status static_sort_scratch(void** out)
+{
+    constexpr int kMaxDevices = 64;
+    static std::mutex mu;
+    static void* addr[kMaxDevices] = {};
+    int dev = 0;
+    PB_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return PICASSO_ERR_NO_DEVICE;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[dev]) {
+        void* p = nullptr;
+        PB_CUDA_TRY(cudaGetSymbolAddress(&p, g_sort_scratch));
+        addr[dev] = p;
+    }
+    *out = addr[dev];
+    return PICASSO_OK;
+}
+
+}  // namespace pb
+
+extern "C" picasso_status picasso_cell_sort_static(const picasso_spline* sd,
+                                                   int64_t num_particles,
+                                                   picasso_particle_field x_p,
+                                                   const int32_t tile[3], int32_t chunk,
+                                                   uint32_t* key, uint32_t* perm,
+                                                   int64_t* tile_offset, uint32_t* tile_items,
+                                                   picasso_bins* bins_out,
+                                                   const picasso_exec* exec)
+{
+    SortPlan pl;
+    picasso_status st = make_plan(sd, num_particles, tile, &pl);
+    if (st) return st;
+    if (pl.bytes > kStaticSortScratchBytes) return PICASSO_ERR_OUT_OF_RANGE;
+    void* ws = nullptr;
+    if ((st = static_sort_scratch(&ws))) return st;
+    // Every scratch word the sort reads is written earlier in the same call,
+    // so nothing needs clearing between calls.
+    return picasso_cell_sort(sd, num_particles, x_p, tile, chunk, key, perm, tile_offset,
+                             tile_items, ws, kStaticSortScratchBytes, bins_out, exec);
 }
