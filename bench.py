@@ -282,6 +282,19 @@ def time_form(step, steps, warmup, dist):
     return ms, per
 
 
+def measured_traffic(kernel, n, form):
+    """DRAM bytes of one launch of a tiled FP32-form kernel, from the ncu
+    capture summarised in profiles/ncu_traffic.json, scaled by the particle
+    count (traffic grows in proportion to the particles processed)."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    name = {"p2g": "p2g_tiled", "g2p": "g2p_tiled"}.get(kernel)
+    if form != "fp32" or name is None or not os.path.exists(path):
+        return None
+    with open(path) as f:
+        t = json.load(f)
+    return t[name]["dram_bytes_per_particle"] * n if name in t else None
+
+
 def roofline(step, per_ms, n, nodes, peak):
     kb = step.kernel_bytes(n, nodes)
     dom = max(per_ms, key=lambda k: per_ms[k])
@@ -291,7 +304,9 @@ def roofline(step, per_ms, n, nodes, peak):
                for k in per_ms}
     return {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak["hbm_gbs"],
             "unit": "GB/s", "frac": ach / peak["hbm_gbs"],
-            "peak_source": peak["source"], "traffic": None}, kernels
+            "peak_source": peak["source"],
+            "traffic": measured_traffic(dom, n, step.form) if step.bins is not None else None,
+            "algorithmic_bytes": kb[dom]}, kernels
 
 
 def run_ours(args):

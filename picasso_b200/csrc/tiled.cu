@@ -31,7 +31,11 @@ constexpr int kStageLanes = 8;     // lanes staged per merge round
 constexpr int kStageStride = 116;  // floats per staged lane (4 fields x 28 + pad;
                                    // 116 mod 32 = 20 keeps 8 float4 stores apart)
 constexpr int kRing = 3;           // particles in flight per lane
-constexpr int kSlot = 28;          // floats per ring slot: x (6) | pad (2) | c (12) | m (1) | pad
+// ring of particle records, one slot per lane and stage, in three arrays so
+// that every access pattern is free of bank conflicts: x (3 doubles, 6-word
+// lane stride), c (12 floats, 12-word stride), m (1 float)
+constexpr int kRingX = 6, kRingC = 12;
+constexpr int kRingFloats = 32 * (kRingX + kRingC + 1);
 constexpr unsigned kFull = 0xFFFFFFFFu;
 
 struct TileP {
@@ -306,8 +310,8 @@ p2g_tiled_kernel(MeshP mp, TileP tp, int64_t n, const double* __restrict__ xg,
     extern __shared__ __align__(16) float smem[];
     __shared__ int stage_base[kStageLanes];
     const int lane = threadIdx.x;
-    float* ring = smem;
-    float* stage = ring + kRing * 32 * kSlot;
+    float* ring = smem;  // [kRing][x: 32*6 | c: 32*12 | m: 32]
+    float* stage = ring + kRing * kRingFloats;
     float* tile = stage + kStageLanes * kStageStride;
 
     if (blockIdx.x == 0 && threadIdx.x == 0 && err) {
@@ -327,18 +331,25 @@ p2g_tiled_kernel(MeshP mp, TileP tp, int64_t n, const double* __restrict__ xg,
     plan.init(tp, lane);
     const float D = (ORDER >= 2) ? inertial_scaling<ORDER, float>(mp.dx[0]) : 0.f;
 
-    float* myring = ring + lane * kSlot;  // slot q at myring + q * 32 * kSlot
+    auto slot_x = [&](int q) { return ring + (q % kRing) * kRingFloats + lane * kRingX; };
+    auto slot_c = [&](int q) {
+        return ring + (q % kRing) * kRingFloats + 32 * kRingX + lane * kRingC;
+    };
+    auto slot_m = [&](int q) {
+        return ring + (q % kRing) * kRingFloats + 32 * (kRingX + kRingC) + lane;
+    };
     auto issue = [&](int q) {
         if (q < cnt) {
             const int64_t p = my0 + q;
-            float* s = myring + (q % kRing) * 32 * kSlot;
-            cp_async<8>(s + 0, xg + 3 * p + 0);
-            cp_async<8>(s + 2, xg + 3 * p + 1);
-            cp_async<8>(s + 4, xg + 3 * p + 2);
-            cp_async<16>(s + 8, cg + 12 * p + 0);
-            cp_async<16>(s + 12, cg + 12 * p + 4);
-            cp_async<16>(s + 16, cg + 12 * p + 8);
-            cp_async<4>(s + 20, mg + p);
+            float* sx = slot_x(q);
+            float* sc = slot_c(q);
+            cp_async<8>(sx + 0, xg + 3 * p + 0);
+            cp_async<8>(sx + 2, xg + 3 * p + 1);
+            cp_async<8>(sx + 4, xg + 3 * p + 2);
+            cp_async<16>(sc + 0, cg + 12 * p + 0);
+            cp_async<16>(sc + 4, cg + 12 * p + 4);
+            cp_async<16>(sc + 8, cg + 12 * p + 8);
+            cp_async<4>(slot_m(q), mg + p);
         }
         cp_async_commit();
     };
@@ -360,20 +371,20 @@ p2g_tiled_kernel(MeshP mp, TileP tp, int64_t n, const double* __restrict__ xg,
         bool ok = false;
         float cp[12], mass = 0.f;
         if (valid) {
-            const float* sl = myring + (s % kRing) * 32 * kSlot;
-            const double2 x01 = *reinterpret_cast<const double2*>(sl);
-            const double xp[3] = {x01.x, x01.y, *reinterpret_cast<const double*>(sl + 4)};
+            const double* sx = reinterpret_cast<const double*>(slot_x(s));
+            const double xp[3] = {sx[0], sx[1], sx[2]};
             ok = locate<ORDER>(mp, tp, xp, ob, sp, lb);
             if (!ok && err) atomicAdd(err, 1);
+            const float* sc = slot_c(s);
 #pragma unroll
             for (int q = 0; q < 3; ++q) {
-                const float4 v = *reinterpret_cast<const float4*>(sl + 8 + 4 * q);
+                const float4 v = *reinterpret_cast<const float4*>(sc + 4 * q);
                 cp[4 * q] = v.x;
                 cp[4 * q + 1] = v.y;
                 cp[4 * q + 2] = v.z;
                 cp[4 * q + 3] = v.w;
             }
-            mass = sl[20];
+            mass = *slot_m(s);
         }
         const int lbin = ok ? (lb[0] * tp.T[1] + lb[1]) * tp.T[2] + lb[2] : -1;
         const unsigned fm = __ballot_sync(kFull, ok && cur >= 0 && lbin != cur);
@@ -485,8 +496,22 @@ g2p_tiled_kernel(MeshP mp, TileP tp, int64_t n, const double* __restrict__ xg, G
         tile[(i * tp.NT[1] + j) * tp.NT[2] + k] = v;
     }
     __syncthreads();
+    // positions are prefetched one particle ahead
+    double xn[3] = {0.0, 0.0, 0.0};
+    if (a + threadIdx.x < b) {
+        const int64_t p0 = a + threadIdx.x;
+        xn[0] = xg[3 * p0];
+        xn[1] = xg[3 * p0 + 1];
+        xn[2] = xg[3 * p0 + 2];
+    }
     for (int64_t p = a + threadIdx.x; p < b; p += kWarps * 32) {
-        const double xp[3] = {xg[3 * p], xg[3 * p + 1], xg[3 * p + 2]};
+        const double xp[3] = {xn[0], xn[1], xn[2]};
+        const int64_t pn = p + kWarps * 32;
+        if (pn < b) {
+            xn[0] = xg[3 * pn];
+            xn[1] = xg[3 * pn + 1];
+            xn[2] = xg[3 * pn + 2];
+        }
         Spline1D<ORDER, float> sp[3];
         int lb[3];
         if (!locate<ORDER>(mp, tp, xp, ob, sp, lb) || lb[0] < i_lo || lb[0] > i_hi) {
@@ -659,7 +684,7 @@ template <int ORDER>
 static size_t p2g_smem(const TileP& tp)
 {
     return sizeof(float) *
-           ((size_t)kRing * 32 * kSlot + kStageLanes * kStageStride + 4 * (size_t)tp.P);
+           ((size_t)kRing * kRingFloats + kStageLanes * kStageStride + 4 * (size_t)tp.P);
 }
 
 template <int ORDER>
