@@ -48,6 +48,9 @@ def parse():
     ap.add_argument("--order", type=int, default=2)
     ap.add_argument("--workload", default="clustered", choices=["clustered", "uniform"])
     ap.add_argument("--tile", type=int, nargs=3, default=[4, 8, 8])
+    ap.add_argument("--chunk", type=int, default=2048, help="particles per work item")
+    ap.add_argument("--p2g-lanes", type=int, default=0,
+                    help="lanes per particle of the tiled P2G (0 = library choice)")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 plain leg")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -55,6 +58,13 @@ def parse():
                     help="keep the generated particle order (plain kernels)")
     ap.add_argument("--cpu-sample-grid", type=int, default=64)
     ap.add_argument("--json-out", default=None)
+    ap.add_argument("--suite", default="step", choices=["step", "batch"],
+                    help="step: the APIC step on one mesh; batch: many independent instances")
+    ap.add_argument("--batch-instances", type=int, default=512)
+    ap.add_argument("--batch-seed", type=int, default=4)
+    ap.add_argument("--batch-forms", default="fp32,fp64")
+    ap.add_argument("--batch-max-tile-bins", type=int, default=256,
+                    help="largest tile (bins) the batch autotuner may pick")
     return ap.parse_args()
 
 
@@ -179,7 +189,8 @@ def config_of(args):
                         % (args.order, args.grid, args.ppc, args.workload),
             "grid": args.grid, "ppc": args.ppc, "order": args.order,
             "particles": args.grid ** 3 * args.ppc, "positions": args.workload,
-            "tile": list(args.tile), "l2": "inputs >> 126 MB L2 (no flush needed)",
+            "tile": list(args.tile), "chunk": args.chunk, "p2g_lanes": args.p2g_lanes,
+            "l2": "inputs >> 126 MB L2 (no flush needed)",
             "parallelism": "replicas"}
 
 
@@ -343,7 +354,8 @@ def run_ours(args):
             torch.cuda.synchronize()
             e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
             e0.record()
-            key, perm, bins = pb.cell_sort(sd0, tuple(args.tile))
+            key, perm, bins = pb.cell_sort(sd0, tuple(args.tile), chunk=args.chunk,
+                                           p2g_lanes=args.p2g_lanes)
             e1.record()
             xs, ms_, cs = pb.permute_members(perm, x, m64, c64)
             e2.record()
@@ -479,10 +491,179 @@ def run_e2e(step, x, m32, c32, args, stream, dist, world):
             "path": "torch pinned copies + C-ABI transfer calls"}
 
 
+# ---------------------------------------------------------------------------
+# batched independent instances
+# ---------------------------------------------------------------------------
+BATCH_METRIC = ("batched APIC step particles/s: independent instances, edges 16..96 step 8, "
+                "1-16 ppc, quadratic/cubic, one persistent launch per step vs sequential "
+                "single launches")
+
+
+def batch_shapes(count, seed):
+    """(edge, particles per cell, order) of every instance: edge uniform in
+    {16, 24, ..., 96}, particles per cell uniform in 1..16, order 2 or 3."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    edges = rng.choice(np.arange(16, 97, 8), count)
+    ppcs = rng.integers(1, 17, count)
+    orders = rng.choice([2, 3], count)
+    return [(int(e), int(p), int(o)) for e, p, o in zip(edges, ppcs, orders)]
+
+
+def batch_bytes(shapes, f32):
+    """Algorithmic HBM bytes of one batched step (the per-kernel model of the
+    single-mesh step, summed over instances)."""
+    sf, su = (4, 4) if f32 else (8, 8)
+    total = 0
+    for e, p, _ in shapes:
+        n, nodes = e ** 3 * p, e ** 3
+        total += nodes * 32                                   # fill
+        total += n * (24 + 13 * sf) + nodes * 32              # p2g
+        total += nodes * (32 + 3 * su)                        # velocity
+        total += n * (24 + 12 * sf) + nodes * 3 * su          # g2p
+    return total
+
+
+def run_batch(args):
+    import torch
+
+    import picasso_b200 as pb
+    from picasso_b200 import autotune, workloads
+
+    torch.cuda.set_device(0)
+    peak = peaks()
+    shapes = batch_shapes(args.batch_instances, args.batch_seed)
+    out = {"metric": BATCH_METRIC, "unit": "particles/s", "n_gpus": 1, "steps": args.steps,
+           "warmup": args.warmup, "higher_is_better": True, "data": "synthetic",
+           "config": {"workload": "%d independent APIC instances, edge uniform in "
+                                  "{16,24,...,96}, 1-16 ppc, order 2 or 3 per instance, uniform "
+                                  "positions" % len(shapes),
+                      "instances": len(shapes), "seed": args.batch_seed,
+                      "particles": sum(e ** 3 * p for e, p, _ in shapes),
+                      "nodes": sum(e ** 3 for e, _, _ in shapes),
+                      "quadratic": sum(1 for s in shapes if s[2] == 2),
+                      "cubic": sum(1 for s in shapes if s[2] == 3),
+                      "l2": "inputs >> 126 MB L2 (no flush needed)"},
+           "forms": {}}
+    tuner = autotune.Tuner(fixed_bits=FIXED_BITS, batched=True,
+                           max_tile_bins=args.batch_max_tile_bins)
+    clocks = Clocks(0)
+    clocks.start()
+    for form in args.batch_forms.split(","):
+        f32 = form == "fp32"
+        t0 = time.time()
+        tuner.tune_shapes(shapes, f32)
+        tune_s = time.time() - t0
+        per_particle = 24 + (52 if f32 else 104)
+        per_node = (32 + 12) if f32 else (32 + 24)
+        # instances in groups that fit in 80 % of the free memory; each group
+        # is one batch, the step time of all instances is the sum over groups
+        budget = 0.8 * torch.cuda.mem_get_info()[0]
+        groups, cur, cur_b = [], [], 0
+        for i, (e, p, o) in enumerate(shapes):
+            need = e ** 3 * p * per_particle + e ** 3 * per_node
+            if cur and cur_b + need > budget:
+                groups.append(cur)
+                cur, cur_b = [], 0
+            cur.append(i)
+            cur_b += need
+        groups.append(cur)
+        pdt = torch.float32 if f32 else torch.float64
+        n_total = sum(e ** 3 * p for e, p, _ in shapes)
+        nbytes = batch_bytes(shapes, f32)
+        res = {"instances": len(shapes), "particles": n_total, "tune_s": tune_s,
+               "groups": len(groups), "algorithmic_bytes": nbytes, "modes": {}}
+        acc_ms = {"fused": 0.0, "phased": 0.0, "sequential": 0.0}
+        infos = {}
+        for grp in groups:
+            insts = []
+            for i in grp:
+                e, p, o = shapes[i]
+                ch = tuner.choice(o, e, p, f32)
+                mesh = pb.UniformMesh([0, 0, 0, 1, 1, 1], cell_size=1.0 / e,
+                                      periodic=(True,) * 3)
+                x = workloads.positions("uniform", e, p, seed=1000 + i)
+                m, c = workloads.particle_state(x.shape[0], 1000 + i, dtype=pdt)
+                loc = pb.FieldLocation.Node
+                sd0 = pb.create_spline(loc, o, mesh, x)
+                _, perm, bins = pb.cell_sort(sd0, tuple(ch["tile"]), chunk=ch["chunk"],
+                                             p2g_lanes=ch["lanes"])
+                x, m, c = pb.permute_members(perm, x, m, c.contiguous())
+                del perm, sd0
+                sd = pb.create_spline(loc, o, mesh, x)
+                ext = mesh.extent(loc)
+                if f32:
+                    acc = torch.zeros(ext + (4,), dtype=torch.int64, device="cuda")
+                    gm = pb.FixedGrid(acc[..., 0], FIXED_BITS)
+                    gmu = pb.FixedGrid(acc[..., 1:], FIXED_BITS)
+                    u = torch.zeros(ext + (3,), dtype=torch.float32, device="cuda")
+                else:
+                    acc = torch.zeros(ext + (4,), dtype=torch.float64, device="cuda")
+                    gm, gmu = acc[..., 0], acc[..., 1:]
+                    u = torch.zeros(ext + (3,), dtype=torch.float64, device="cuda")
+                insts.append(pb.BatchInstance(sd, m, c, gm, gmu, u, bins, 1e-12))
+            torch.cuda.synchronize()
+            for mode in ("fused", "phased", "sequential"):
+                b = pb.Batch(insts, mode="phased" if mode == "sequential" else mode)
+                if mode == "sequential":
+                    run = b.step_sequential
+                else:
+                    def run(b=b):
+                        b.step(graph=True)
+                for _ in range(args.warmup):
+                    run()
+                torch.cuda.synchronize()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record()
+                for _ in range(args.steps):
+                    run()
+                e1.record()
+                torch.cuda.synchronize()
+                acc_ms[mode] += e0.elapsed_time(e1) / args.steps
+                b.status()
+                infos.setdefault(mode, []).append(b.info())
+                b.close()
+            del insts
+            torch.cuda.synchronize()
+            torch.cuda.empty_cache()
+        for mode, ms in acc_ms.items():
+            gbs = nbytes / (ms * 1e-3) / 1e9
+            launches = {"fused": 1, "phased": 4, "sequential": 5 * len(shapes) // len(groups)}
+            res["modes"][mode] = {"ms_per_step": ms, "particles_per_s": n_total / (ms * 1e-3),
+                                  "gbs": gbs, "frac_hbm": gbs / peak["hbm_gbs"],
+                                  "launches_per_step": launches[mode] * len(groups),
+                                  "grid_blocks": [i["grid_blocks"] for i in infos[mode]],
+                                  "smem_bytes": [i["smem_bytes"] for i in infos[mode]]}
+        seq = res["modes"]["sequential"]["ms_per_step"]
+        for mode in ("fused", "phased"):
+            res["modes"][mode]["speedup_vs_sequential"] = seq / res["modes"][mode]["ms_per_step"]
+        res["tuned"] = {k: v for k, v in tuner.table.items() if ("f32" if f32 else "f64") in k}
+        res["tuned_classes"] = len(res["tuned"])
+        out["forms"][form] = res
+    out["clocks"] = clocks.stop()
+    best = out["forms"].get("fp32", next(iter(out["forms"].values())))
+    out["value"] = best["modes"]["fused"]["particles_per_s"]
+    out["ms_per_step"] = best["modes"]["fused"]["ms_per_step"]
+    out["dtype"] = "f32 (i64 fixed-point grid)" if "fp32" in out["forms"] else "f64"
+    out["roofline"] = {"bound": "hbm", "achieved": best["modes"]["fused"]["gbs"],
+                       "peak": peak["hbm_gbs"], "unit": "GB/s",
+                       "frac": best["modes"]["fused"]["frac_hbm"],
+                       "peak_source": peak["source"], "traffic": None}
+    out["autotune_measurements"] = tuner.measurements
+    line = json.dumps(out)
+    print(line)
+    if args.json_out:
+        with open(args.json_out, "w") as f:
+            f.write(line + "\n")
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.suite == "batch":
+        run_batch(args)
     else:
         run_ours(args)
 

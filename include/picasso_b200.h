@@ -142,6 +142,10 @@ typedef struct picasso_bins {
     int32_t order;               /* spline order the bins were built for */
     int32_t location;            /* picasso_location the bins were built for */
     int32_t chunk;               /* particles per work item */
+    int32_t p2g_lanes;           /* lanes per particle of the tiled P2G: 1, 2 or
+                                    4 for orders 1-2, 4 for order 3 (the 4 grid
+                                    fields are split between them); 0 = the
+                                    library's choice; set to 0 by the sort */
     const int64_t* tile_offset;  /* device, num_tiles_total + 1 particle offsets */
     const uint32_t* tile_items;  /* device, num_tiles_total + 1: first work item
                                     of each tile (exclusive prefix of
@@ -321,6 +325,78 @@ PICASSO_API picasso_status picasso_permute(int64_t num_particles, int32_t ncomp,
  * and y != NULL also y = a_inv * x (3-vectors). */
 PICASSO_API picasso_status picasso_mat3_inverse(int64_t n, const double* a, double* a_inv, double* det,
                                     const double* x, double* y, const picasso_exec* exec);
+
+/* ------------------------------------------------------------------------ */
+/* Batched independent APIC problems                                        */
+/* ------------------------------------------------------------------------ */
+/* No counterpart in the reference, which runs one mesh per rank and one
+ * kernel per GridOperator::apply.  A batch holds many independent APIC
+ * problems (meshes of any size, any particle count, order 1-3 each) and runs
+ * one APIC step over all of them -- fill of the scatter fields, P2G, grid
+ * velocity, G2P, i.e. GridOperator.hpp:532 zeroing + APIC.hpp:55-140 +
+ * v = p / m + APIC.hpp:407-471 per instance -- in persistent kernel launches
+ * that take work items of every instance from one queue. */
+
+typedef struct picasso_batch_instance {
+    picasso_spline spline;          /* collocated NODE location, order 1..3 */
+    int64_t num_particles;
+    picasso_particle_field x_p;     /* packed (n,3) F64 */
+    picasso_particle_field m_p;     /* packed (n): F32 (precision form) or F64 */
+    picasso_particle_field c_p;     /* packed (n,4,3), 16-byte aligned, type of m_p */
+    picasso_grid_field m_i;         /* node mass: I64_FIXED (precision form) or F64 */
+    picasso_grid_field mu_i;        /* node momentum (3 components), type of m_i */
+    picasso_grid_field u_i;         /* node velocity (3 components): F32 or F64 */
+    double mass_threshold;          /* u = mu / m where m > threshold, else 0 */
+    picasso_bins bins;              /* bins of the sorted particles (picasso_cell_sort) */
+    int32_t* error_count;           /* optional device counter (skipped particles) */
+} picasso_batch_instance;
+
+typedef enum picasso_batch_mode {
+    /* one persistent launch per step; an instance's items wait for the
+       instance's previous phase (bounded spin on device counters) */
+    PICASSO_BATCH_FUSED = 0,
+    /* one persistent launch per phase (4 per step), no waits */
+    PICASSO_BATCH_PHASED = 1
+} picasso_batch_mode;
+
+typedef struct picasso_batch_info {
+    int32_t count;            /* instances */
+    int32_t precision_form;   /* 1 = FP32 particles + fixed-point grid, 0 = FP64 */
+    int32_t grid_blocks;      /* persistent CTAs (one warp each) */
+    int32_t smem_bytes;       /* dynamic shared memory per CTA */
+    int64_t items[4];         /* work items per phase: fill, p2g, velocity, g2p */
+    int64_t particles;        /* total particles */
+} picasso_batch_info;
+
+typedef struct picasso_batch picasso_batch;  /* opaque */
+
+/* Validates the instances, copies their descriptors to the device (the
+ * pointed-to arrays are not copied: they must stay valid, and the bins must
+ * keep describing the particles, for the life of the batch) and sizes the
+ * persistent launch.  All instances use the same form: precision form
+ * (F32 m_p, c_p; I64_FIXED m_i, mu_i; F32 u_i) or FP64 (all F64).  Allocates
+ * its device tables here and nowhere else. */
+PICASSO_API picasso_status picasso_batch_create(const picasso_batch_instance* instances,
+                                                int32_t count, int32_t mode,
+                                                picasso_batch** out);
+/* One APIC step of every instance on `stream`.  use_graph != 0 replays a
+ * CUDA graph captured at the first such call (one memset node + the
+ * persistent launches).  Returns PICASSO_ERR_CUDA for launch errors; a wait
+ * that ran out (which the design rules out) is reported by
+ * picasso_batch_status.  Steps of one batch must not overlap on the GPU (they
+ * share the queue counters). */
+PICASSO_API picasso_status picasso_batch_step(picasso_batch* batch, void* stream,
+                                              int32_t use_graph);
+/* The same step issued as single launches, instance after instance
+ * (picasso_grid_fill x 2, picasso_apic_p2g, picasso_grid_velocity,
+ * picasso_apic_g2p): the comparison for the batched launch. */
+PICASSO_API picasso_status picasso_batch_step_sequential(picasso_batch* batch, void* stream);
+/* Synchronises `stream` and returns PICASSO_ERR_TIMEOUT if a dependency wait
+ * of an earlier step ran out of polls (and clears that flag), else PICASSO_OK. */
+PICASSO_API picasso_status picasso_batch_status(picasso_batch* batch, void* stream);
+PICASSO_API picasso_status picasso_batch_get_info(const picasso_batch* batch,
+                                                  picasso_batch_info* info);
+PICASSO_API picasso_status picasso_batch_destroy(picasso_batch* batch);
 
 #ifdef __cplusplus
 }

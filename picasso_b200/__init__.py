@@ -10,6 +10,8 @@ not been built.
 from ._abi import PicassoError, load_library  # noqa: F401
 from .api import (  # noqa: F401
     APIC,
+    Batch,
+    BatchInstance,
     Bins,
     Exec,
     FieldLocation,

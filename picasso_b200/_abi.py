@@ -57,13 +57,29 @@ class GridField(C.Structure):
 class Bins(C.Structure):
     _fields_ = [("tile", C.c_int32 * 3), ("num_tiles", C.c_int32 * 3),
                 ("bin_extent", C.c_int32 * 3), ("order", C.c_int32), ("location", C.c_int32),
-                ("chunk", C.c_int32), ("tile_offset", C.c_void_p), ("tile_items", C.c_void_p)]
+                ("chunk", C.c_int32), ("p2g_lanes", C.c_int32), ("tile_offset", C.c_void_p),
+                ("tile_items", C.c_void_p)]
 
 
 class Exec(C.Structure):
     _fields_ = [("stream", C.c_void_p), ("error_count", C.c_void_p),
                 ("bins", C.POINTER(Bins))]
 
+
+class BatchInstance(C.Structure):
+    _fields_ = [("spline", Spline), ("num_particles", C.c_int64), ("x_p", ParticleField),
+                ("m_p", ParticleField), ("c_p", ParticleField), ("m_i", GridField),
+                ("mu_i", GridField), ("u_i", GridField), ("mass_threshold", C.c_double),
+                ("bins", Bins), ("error_count", C.c_void_p)]
+
+
+class BatchInfo(C.Structure):
+    _fields_ = [("count", C.c_int32), ("precision_form", C.c_int32),
+                ("grid_blocks", C.c_int32), ("smem_bytes", C.c_int32),
+                ("items", C.c_int64 * 4), ("particles", C.c_int64)]
+
+
+BATCH_FUSED, BATCH_PHASED = 0, 1
 
 # (name, restype, argtypes) of every entry point in the header
 SIGNATURES = [
@@ -103,6 +119,13 @@ SIGNATURES = [
     ("picasso_mat3_inverse", C.c_int,
      [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
       C.POINTER(Exec)]),
+    ("picasso_batch_create", C.c_int,
+     [C.POINTER(BatchInstance), C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]),
+    ("picasso_batch_step", C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
+    ("picasso_batch_step_sequential", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("picasso_batch_status", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("picasso_batch_get_info", C.c_int, [C.c_void_p, C.POINTER(BatchInfo)]),
+    ("picasso_batch_destroy", C.c_int, [C.c_void_p]),
 ]
 
 _lib = None

@@ -390,11 +390,12 @@ class Bins:
         return self.desc.num_tiles[0] * self.desc.num_tiles[1] * self.desc.num_tiles[2]
 
 
-def cell_sort(sd, tile=(4, 8, 8), chunk=2048, stream=None, workspace=None):
+def cell_sort(sd, tile=(4, 8, 8), chunk=2048, stream=None, workspace=None, p2g_lanes=0):
     """Stable sort of the spline's particles by (tile, bin).  Returns
     (key, perm, bins): keys and permutation as int32 tensors holding uint32
     values, and the Bins to pass to the transfers once the particle members
-    have been permuted (see permute / permute_members)."""
+    have been permuted (see permute / permute_members).  `p2g_lanes` (1, 2, 4;
+    0 = library choice) is the tiled P2G's lanes per particle."""
     lib = _lib()
     n = sd.num_particles
     t3 = (C.c_int32 * 3)(*tile)
@@ -419,6 +420,7 @@ def cell_sort(sd, tile=(4, 8, 8), chunk=2048, stream=None, workspace=None):
                                 key.data_ptr(), perm.data_ptr(), tile_offset.data_ptr(),
                                 tile_items.data_ptr(), workspace.data_ptr(), workspace.numel(),
                                 C.byref(bins), C.byref(ex.desc)), "cell_sort")
+    bins.p2g_lanes = int(p2g_lanes)
     return key[:n], perm[:n], Bins(bins, tile_offset, tile_items)
 
 
@@ -458,6 +460,91 @@ def mat3_inverse(a, x=None, stream=None):
                                       y.data_ptr() if y is not None else None, C.byref(ex.desc)),
           "mat3_inverse")
     return (inv, det, y) if x is not None else (inv, det)
+
+
+# ---------------------------------------------------------------------------
+# batched independent instances
+# ---------------------------------------------------------------------------
+
+
+class BatchInstance:
+    """One APIC problem of a :class:`Batch`: its spline (collocated Node
+    mesh and order), packed particle members sorted with :func:`cell_sort`
+    (x (N, 3) FP64, m (N), c (N, 4, 3)), its grid arrays and its bins.
+    Precision form: m, c float32, m_i / mu_i FixedGrid, u_i float32; FP64
+    form: all float64."""
+
+    def __init__(self, sd, m_p, c_p, m_i, mu_i, u_i, bins, mass_threshold=1e-12,
+                 error_count=None):
+        d = _abi.BatchInstance()
+        d.spline = sd.desc
+        d.num_particles = sd.num_particles
+        d.x_p = particle_field(sd.x)
+        d.m_p = particle_field(m_p)
+        d.c_p = particle_field(c_p)
+        d.m_i = grid_field(m_i)
+        d.mu_i = grid_field(mu_i)
+        d.u_i = grid_field(u_i)
+        d.mass_threshold = float(mass_threshold)
+        d.bins = bins.desc
+        d.error_count = error_count.data_ptr() if error_count is not None else None
+        self.desc = d
+        # the batch reads these arrays at every step
+        self._keep = (sd, m_p, c_p, m_i, mu_i, u_i, bins, error_count)
+
+
+class Batch:
+    """Many independent APIC problems stepped together: fill, P2G, grid
+    velocity and G2P of every instance in persistent launches fed by one
+    work queue (``mode="fused"``: one launch per step; ``"phased"``: one
+    launch per phase).  ``step(graph=True)`` replays a captured CUDA graph.
+    ``step_sequential`` issues the same work as single calls, instance after
+    instance."""
+
+    MODES = {"fused": _abi.BATCH_FUSED, "phased": _abi.BATCH_PHASED}
+
+    def __init__(self, instances, mode="fused"):
+        self.instances = list(instances)
+        arr = (_abi.BatchInstance * len(self.instances))(*[i.desc for i in self.instances])
+        h = C.c_void_p()
+        check(_lib().picasso_batch_create(arr, len(self.instances), self.MODES[mode],
+                                          C.byref(h)), "batch_create")
+        self._h = h
+        self.mode = mode
+
+    def _stream(self, stream):
+        s = stream if stream is not None else torch.cuda.current_stream()
+        return s.cuda_stream
+
+    def step(self, stream=None, graph=True):
+        check(_lib().picasso_batch_step(self._h, self._stream(stream), int(bool(graph))),
+              "batch_step")
+
+    def step_sequential(self, stream=None):
+        check(_lib().picasso_batch_step_sequential(self._h, self._stream(stream)),
+              "batch_step_sequential")
+
+    def status(self, stream=None):
+        """Synchronises the stream; raises if a dependency wait ran out."""
+        check(_lib().picasso_batch_status(self._h, self._stream(stream)), "batch_status")
+
+    def info(self):
+        inf = _abi.BatchInfo()
+        check(_lib().picasso_batch_get_info(self._h, C.byref(inf)), "batch_get_info")
+        return {"count": inf.count, "precision_form": bool(inf.precision_form),
+                "grid_blocks": inf.grid_blocks, "smem_bytes": inf.smem_bytes,
+                "items": list(inf.items), "particles": inf.particles}
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            _lib().picasso_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def fixed_bits_for(max_abs):

@@ -3,42 +3,9 @@
 // near-empty-node threshold, and the FP64 particle position update.
 #include <cmath>
 
-#include "common.cuh"
+#include "gridops.cuh"
 
 namespace pb {
-
-struct Box {
-    int lo[3];
-    int n[3];
-    __host__ __device__ int64_t count() const { return (int64_t)n[0] * n[1] * n[2]; }
-    __device__ __forceinline__ void at(int64_t e, int& i, int& j, int& k) const
-    {
-        k = lo[2] + (int)(e % n[2]);
-        e /= n[2];
-        j = lo[1] + (int)(e % n[1]);
-        i = lo[0] + (int)(e / n[1]);
-    }
-};
-
-static Box full_box(const picasso_mesh& m)
-{
-    Box b;
-    for (int d = 0; d < 3; ++d) {
-        b.lo[d] = 0;
-        b.n[d] = m.extent[d];
-    }
-    return b;
-}
-
-static Box owned_box(const picasso_mesh& m)
-{
-    Box b;
-    for (int d = 0; d < 3; ++d) {
-        b.lo[d] = m.periodic[d] ? m.own_begin[d] : 0;
-        b.n[d] = m.periodic[d] ? m.own_extent[d] : m.extent[d];
-    }
-    return b;
-}
 
 template <class T>
 __global__ void fill_kernel(Box b, GField f, int ncomp, T v)
@@ -52,14 +19,6 @@ __global__ void fill_kernel(Box b, GField f, int ncomp, T v)
     }
 }
 
-template <class T>
-__device__ __forceinline__ double load_value(const GField& f, int i, int j, int k, int c,
-                                             double scale_inv)
-{
-    return (double)*f.ptr<T>(i, j, k, c) * scale_inv;
-}
-
-// u = mu / m where m > threshold else 0; all arithmetic in FP64.
 template <class MT, class UT, int NC>
 __global__ void velocity_kernel(Box b, GField gm, GField gmu, GField gu, GField gu64,
                                 double thr, double inv_m, double inv_mu)
@@ -69,14 +28,7 @@ __global__ void velocity_kernel(Box b, GField gm, GField gmu, GField gu, GField 
          e += (int64_t)gridDim.x * blockDim.x) {
         int i, j, k;
         b.at(e, i, j, k);
-        const double m = load_value<MT>(gm, i, j, k, 0, inv_m);
-        const bool keep = m > thr;
-#pragma unroll
-        for (int c = 0; c < NC; ++c) {
-            const double v = keep ? load_value<MT>(gmu, i, j, k, c, inv_mu) / m : 0.0;
-            *gu.ptr<UT>(i, j, k, c) = (UT)v;
-            if (gu64.data) *gu64.ptr<double>(i, j, k, c) = v;
-        }
+        velocity_node<MT, UT, NC>(gm, gmu, gu, gu64, i, j, k, thr, inv_m, inv_mu);
     }
 }
 

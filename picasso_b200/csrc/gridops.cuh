@@ -1,0 +1,63 @@
+// Per-node bodies of the grid operations between P2G and G2P: the node box
+// iterated by the grid kernels (grid.cu, batch.cu) and the FP64
+// momentum-to-velocity update with the near-empty-node threshold.
+#pragma once
+
+#include "common.cuh"
+
+namespace pb {
+
+struct Box {
+    int lo[3];
+    int n[3];
+    __host__ __device__ int64_t count() const { return (int64_t)n[0] * n[1] * n[2]; }
+    __device__ __forceinline__ void at(int64_t e, int& i, int& j, int& k) const
+    {
+        k = lo[2] + (int)(e % n[2]);
+        e /= n[2];
+        j = lo[1] + (int)(e % n[1]);
+        i = lo[0] + (int)(e / n[1]);
+    }
+};
+
+// All entities of the local grid (the fill range).
+inline Box full_box(const picasso_mesh& m)
+{
+    Box b;
+    for (int d = 0; d < 3; ++d) {
+        b.lo[d] = 0;
+        b.n[d] = m.extent[d];
+    }
+    return b;
+}
+
+// Nodes a periodic mesh owns (non-periodic: all entities); the velocity range.
+inline Box owned_box(const picasso_mesh& m)
+{
+    Box b;
+    for (int d = 0; d < 3; ++d) {
+        b.lo[d] = m.periodic[d] ? m.own_begin[d] : 0;
+        b.n[d] = m.periodic[d] ? m.own_extent[d] : m.extent[d];
+    }
+    return b;
+}
+
+// u = mu / m where m > threshold else 0; all arithmetic in FP64.  CG loads
+// the accumulators through L2 only (grids written earlier in the same launch).
+template <class MT, class UT, int NC, bool CG = false>
+__device__ __forceinline__ void velocity_node(const GField& gm, const GField& gmu,
+                                              const GField& gu, const GField& gu64, int i, int j,
+                                              int k, double thr, double inv_m, double inv_mu)
+{
+    auto load = [](const MT* a) { return CG ? __ldcg(a) : *a; };
+    const double m = (double)load(gm.ptr<MT>(i, j, k, 0)) * inv_m;
+    const bool keep = m > thr;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        const double v = keep ? (double)load(gmu.ptr<MT>(i, j, k, c)) * inv_mu / m : 0.0;
+        *gu.ptr<UT>(i, j, k, c) = (UT)v;
+        if (gu64.data) *gu64.ptr<double>(i, j, k, c) = v;
+    }
+}
+
+}  // namespace pb

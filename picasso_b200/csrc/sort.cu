@@ -430,6 +430,7 @@ extern "C" picasso_status picasso_cell_sort(const picasso_spline* sd, int64_t nu
         bins_out->order = sd->order;
         bins_out->location = sd->location;
         bins_out->chunk = chunk;
+        bins_out->p2g_lanes = 0;
         bins_out->tile_offset = tile_offset;
         bins_out->tile_items = tile_items;
     }

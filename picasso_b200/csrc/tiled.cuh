@@ -1,0 +1,648 @@
+// Work items of the shared-memory tiled APIC transfers (FP32 precision form)
+// on cell-sorted particles in packed storage: x_p (N,3) FP64, m_p (N) FP32,
+// c_p (N,4,3) FP32.  Used by the single-call kernels (tiled.cu) and by the
+// persistent batched kernel (batch.cu).
+//
+// Work items are chunks of at most `chunk` particles of one tile (the sort
+// writes the per-tile item prefix).
+//
+// P2G item (one warp): particles are processed in runs -- contiguous ranges
+// of the sorted item, so consecutive particles of a run mostly share a
+// stencil -- and each run is handled by LPP lanes (1, 2 or 4) that split the
+// four grid fields (mass, 3 momentum components) between them.  A lane keeps
+// the K^3 sums of its fields for the run's current bin in registers.
+// Particle records arrive through a cp.async ring in shared memory a few
+// particles ahead of use.  When a run's bin changes its lanes stage their
+// partial sums and the warp adds the staged partials into its FP32 node tile
+// ((T + K - 1)^3 nodes) one staged lane after the other: a fixed order without
+// atomics, so the tile sums are reproducible.  At the end of the item the
+// touched box of the tile is rounded to 64-bit fixed point and added to HBM
+// with integer reductions, whose result does not depend on their order; P2G
+// is deterministic for a given particle order.
+//
+// G2P item (one warp or one CTA): the item's node velocities are staged once
+// in a shared float4 tile and every thread gathers its particles' stencils
+// from there, contracting the stencil one dimension at a time.
+#pragma once
+
+#include "common.cuh"
+#include "transfer.cuh"
+
+namespace pb {
+
+constexpr int kStageLanes = 8;  // lanes staged per merge round
+constexpr int kRing = 3;        // particle records in flight per run
+constexpr unsigned kFull = 0xFFFFFFFFu;
+
+struct TileP {
+    int T[3];    // bins per tile
+    int nt[3];   // tiles per dimension
+    int nb[3];   // bins per dimension
+    int NT[3];   // nodes per tile dimension (T + K - 1)
+    int nodes;   // NT0 * NT1 * NT2
+    int SJ, SI;  // P2G node-tile strides along j and i (k stride 1), padded so
+    int P;       // that a merge's stencil nodes hit distinct banks; P = stride
+                 // between the 4 field planes
+    int chunk;
+    int64_t ntiles;
+    const int64_t* off;     // tile particle offsets (ntiles + 1)
+    const uint32_t* items;  // tile work-item prefix (ntiles + 1)
+};
+
+// Per-call (per-instance) arguments of the tiled kernels.
+struct P2GArgs {
+    MeshP mp;
+    TileP tp;
+    const double* x;
+    const float* m;
+    const float* c;
+    GField gm;
+    GField gmu;
+    float scale_m;
+    float scale_mu;
+    int* err;
+};
+
+struct G2PArgs {
+    MeshP mp;
+    TileP tp;
+    const double* x;
+    GField u;
+    float* c;
+    int* err;
+};
+
+__device__ __forceinline__ int bin_of(const MeshP& mp, const TileP& tp, int d, int s0)
+{
+    if (mp.periodic[d]) {
+        const int nb = tp.nb[d];
+        int r = s0 - mp.own_lo[d];
+        if (r < 0) r += nb;          // one period covers every particle inside or
+        else if (r >= nb) r -= nb;   // next to the owned box
+        if ((unsigned)r >= (unsigned)nb) {
+            r %= nb;
+            if (r < 0) r += nb;
+        }
+        return r;
+    }
+    return s0;
+}
+
+__device__ __forceinline__ int node_global(const MeshP& mp, const TileP& tp, int d, int ob,
+                                           int local)
+{
+    int g = ob + local;
+    if (mp.periodic[d]) {
+        if (g >= tp.nb[d]) g -= tp.nb[d];
+        return mp.own_lo[d] + g;
+    }
+    return g;
+}
+
+// Work item w -> tile t and particle range [a, b).  False past the last item.
+__device__ __forceinline__ bool item_range(const TileP& tp, int64_t w, int64_t& t, int64_t& a,
+                                           int64_t& b)
+{
+    if (w >= (int64_t)__ldg(tp.items + tp.ntiles)) return false;
+    int64_t lo = 0, hi = tp.ntiles - 1;  // last t with items[t] <= w
+    while (lo < hi) {
+        const int64_t mid = (lo + hi + 1) >> 1;
+        if ((int64_t)__ldg(tp.items + mid) <= w) lo = mid;
+        else hi = mid - 1;
+    }
+    t = lo;
+    a = __ldg(tp.off + t) + (w - (int64_t)__ldg(tp.items + t)) * tp.chunk;
+    b = min(a + (int64_t)tp.chunk, (int64_t)__ldg(tp.off + t + 1));
+    return a < b;
+}
+
+__device__ __forceinline__ void tile_origin(const TileP& tp, int64_t t, int ob[3])
+{
+    ob[2] = (int)(t % tp.nt[2]) * tp.T[2];
+    ob[1] = (int)((t / tp.nt[2]) % tp.nt[1]) * tp.T[1];
+    ob[0] = (int)(t / ((int64_t)tp.nt[1] * tp.nt[2])) * tp.T[0];
+}
+
+// Spline of a particle at x and its bin inside the tile with bin origin ob;
+// false if the particle is not in this tile (or not in the mesh).
+template <int ORDER>
+__device__ __forceinline__ bool locate(const MeshP& mp, const TileP& tp, const double xp[3],
+                                       const int ob[3], Spline1D<ORDER, float> sp[3], int lb[3])
+{
+    constexpr int K = SplineTraits<ORDER>::K;
+    bool ok = true;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        eval_spline<ORDER>(xp[d], mp.lo[d], mp.dx[d], mp.rdx[d], sp[d]);
+        if (!mp.periodic[d] && (sp[d].s0 < 0 || sp[d].s0 > mp.ext[d] - K)) ok = false;
+        lb[d] = bin_of(mp, tp, d, sp[d].s0) - ob[d];
+        if (lb[d] < 0 || lb[d] >= tp.T[d]) ok = false;
+    }
+    return ok;
+}
+
+// ---------------------------------------------------------------------------
+// cp.async (asynchronous global -> shared copies)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned smem_addr(const void* p)
+{
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* dst, const void* src)
+{
+    if constexpr (BYTES == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_addr(dst)),
+                     "l"(src));
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(smem_addr(dst)),
+                     "l"(src), "n"(BYTES));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait()
+{
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+// ---------------------------------------------------------------------------
+// P2G
+// ---------------------------------------------------------------------------
+// Shared-memory layout of one P2G warp: particle-record ring, staging area,
+// node tile.  Field g of a node (a, b, c) of a bin receives
+//   w_abc * (c0 + cx dist_a + cy dist_b + cz dist_c)        (order 2 / 3)
+//   m * (c0 www + cx gww + cy wgw + cz wwg)                  (order 1)
+// with (c0, cx, cy, cz) = (1, 0, 0, 0) for the mass (g = 0) and
+// (v_d, D B_d0, D B_d1, D B_d2) for momentum component d = g - 1
+// (APIC.hpp:110-139; order 1: APIC.hpp:287-318 with D = 1).
+template <int ORDER, int LPP>
+struct P2GCfg {
+    static constexpr int K = SplineTraits<ORDER>::K;
+    static constexpr int KKK = K * K * K;
+    static constexpr int FS = (KKK + 3) & ~3;  // staged floats per field
+    static constexpr int F = 4 / LPP;          // fields per lane
+    static constexpr int RUNS = 32 / LPP;      // runs per warp
+    static constexpr int SV = F * FS;          // staged values per lane
+    // staging stride: a multiple of 4 floats whose quarter is odd keeps the
+    // float4 stores of 8 staged lanes on distinct banks
+    static constexpr int SS = ((SV / 4) % 2 == 0) ? SV + 4 : SV;
+    static constexpr int R = (SV + 31) / 32;  // merge rounds per staged lane
+    // ring per stage: x (6 floats) | c (12 floats) | m (1 float) per run
+    static constexpr int RING_X = 0, RING_C = 6 * RUNS, RING_M = 18 * RUNS;
+    static constexpr int RING = 19 * RUNS + ((19 * RUNS) % 4 ? 4 - (19 * RUNS) % 4 : 0);
+    static constexpr int STAGE_OFF = kRing * RING;
+    static constexpr int TILE_OFF = STAGE_OFF + kStageLanes * SS;
+    static_assert(LPP == 1 || LPP == 2 || LPP == 4, "1, 2 or 4 lanes per particle");
+};
+
+template <int ORDER, int LPP>
+__host__ __device__ constexpr int p2g_warp_floats(int P)
+{
+    return P2GCfg<ORDER, LPP>::TILE_OFF + 4 * P;
+}
+
+template <int ORDER, int LPP>
+struct P2GAcc {
+    using C = P2GCfg<ORDER, LPP>;
+    float acc[C::F][C::KKK];
+
+    __device__ __forceinline__ void zero()
+    {
+#pragma unroll
+        for (int f = 0; f < C::F; ++f)
+#pragma unroll
+            for (int n = 0; n < C::KKK; ++n) acc[f][n] = 0.f;
+    }
+
+    __device__ __forceinline__ void add(const Spline1D<ORDER, float> sp[3], float mass,
+                                        const float co[C::F][4])
+    {
+        constexpr int K = C::K;
+        if (ORDER >= 2) {
+#pragma unroll
+            for (int i = 0; i < K; ++i)
+#pragma unroll
+                for (int j = 0; j < K; ++j) {
+                    const float wij = sp[0].w[i] * sp[1].w[j] * mass;
+                    float pij[C::F];
+#pragma unroll
+                    for (int f = 0; f < C::F; ++f)
+                        pij[f] = co[f][0] + co[f][1] * sp[0].d[i] + co[f][2] * sp[1].d[j];
+#pragma unroll
+                    for (int k = 0; k < K; ++k) {
+                        const int n = (i * K + j) * K + k;
+                        const float w = wij * sp[2].w[k];
+#pragma unroll
+                        for (int f = 0; f < C::F; ++f) {
+                            if (LPP == 1 && f == 0) acc[f][n] += w;  // mass
+                            else acc[f][n] += w * (pij[f] + co[f][3] * sp[2].d[k]);
+                        }
+                    }
+                }
+        } else {
+#pragma unroll
+            for (int i = 0; i < K; ++i)
+#pragma unroll
+                for (int j = 0; j < K; ++j)
+#pragma unroll
+                    for (int k = 0; k < K; ++k) {
+                        const int n = (i * K + j) * K + k;
+                        const float www = sp[0].w[i] * sp[1].w[j] * sp[2].w[k] * mass;
+                        const float gww = sp[0].g[i] * sp[1].w[j] * sp[2].w[k] * mass;
+                        const float wgw = sp[0].w[i] * sp[1].g[j] * sp[2].w[k] * mass;
+                        const float wwg = sp[0].w[i] * sp[1].w[j] * sp[2].g[k] * mass;
+#pragma unroll
+                        for (int f = 0; f < C::F; ++f) {
+                            if (LPP == 1 && f == 0) acc[f][n] += www;  // mass
+                            else
+                                acc[f][n] += co[f][0] * www + co[f][1] * gww + co[f][2] * wgw +
+                                             co[f][3] * wwg;
+                        }
+                    }
+        }
+    }
+
+    // st[f * FS + n] <- acc[f][n] with 16-byte stores.
+    __device__ __forceinline__ void stage(float* st) const
+    {
+#pragma unroll
+        for (int f = 0; f < C::F; ++f)
+#pragma unroll
+            for (int q = 0; q < C::FS / 4; ++q) {
+                float4 v;
+                v.x = (4 * q + 0 < C::KKK) ? acc[f][4 * q + 0] : 0.f;
+                v.y = (4 * q + 1 < C::KKK) ? acc[f][4 * q + 1] : 0.f;
+                v.z = (4 * q + 2 < C::KKK) ? acc[f][4 * q + 2] : 0.f;
+                v.w = (4 * q + 3 < C::KKK) ? acc[f][4 * q + 3] : 0.f;
+                *reinterpret_cast<float4*>(st + f * C::FS + 4 * q) = v;
+            }
+    }
+};
+
+// Merge plan of one lane: staged value v = lane + 32 r of a staged lane that
+// handles fields hh F .. hh F + F - 1 lands at tile offset
+// moff[r] + hh * fstride from the stencil start.
+template <int ORDER, int LPP>
+struct MergePlan {
+    using C = P2GCfg<ORDER, LPP>;
+    int moff[C::R];
+    int fstride;     // F * P
+    unsigned valid;  // bit r: value lane + 32 r exists
+    __device__ __forceinline__ void init(const TileP& tp, int lane)
+    {
+        constexpr int K = C::K;
+        valid = 0;
+        fstride = C::F * tp.P;
+#pragma unroll
+        for (int r = 0; r < C::R; ++r) {
+            const int v = lane + 32 * r;
+            const int fs = v / C::FS, nn = v - (v / C::FS) * C::FS;
+            moff[r] = 0;
+            if (v < C::SV && nn < C::KKK) {
+                const int a = nn / (K * K), b = (nn / K) % K, c = nn % K;
+                moff[r] = fs * tp.P + a * tp.SI + b * tp.SJ + c;
+                valid |= 1u << r;
+            }
+        }
+    }
+};
+
+// Lanes in `mask` hand their partial sums to the warp's node tile in lane
+// order; their accumulators are zeroed.
+template <int ORDER, int LPP>
+__device__ __forceinline__ void merge_partials(unsigned mask, P2GAcc<ORDER, LPP>& acc,
+                                               int cur_base, const MergePlan<ORDER, LPP>& plan,
+                                               float* tile, float* stage, int* stage_base,
+                                               int lane)
+{
+    using C = P2GCfg<ORDER, LPP>;
+    while (mask) {
+        unsigned batch = mask;
+        if (__popc(mask) > kStageLanes) {  // the lowest kStageLanes lanes
+            batch = 0;
+            unsigned mm = mask;
+#pragma unroll
+            for (int q = 0; q < kStageLanes; ++q) {
+                batch |= mm & (~mm + 1u);
+                mm &= mm - 1u;
+            }
+        }
+        mask &= ~batch;
+        if ((batch >> lane) & 1u) {
+            const int slot = __popc(batch & ((1u << lane) - 1u));
+            acc.stage(stage + slot * C::SS);
+            stage_base[slot] = cur_base | ((lane % LPP) << 28);
+            acc.zero();
+        }
+        __syncwarp();
+        const int nstage = __popc(batch);
+        for (int q = 0; q < nstage; ++q) {
+            const float* st = stage + q * C::SS;
+            const int sb = stage_base[q];
+            const int base = (sb & 0x0FFFFFFF) + (LPP > 1 ? (sb >> 28) * plan.fstride : 0);
+#pragma unroll
+            for (int r = 0; r < C::R; ++r)
+                if ((plan.valid >> r) & 1u) tile[base + plan.moff[r]] += st[lane + 32 * r];
+            __syncwarp();
+        }
+    }
+}
+
+// One P2G work item (tile t, particles [a, b)) by the calling warp.  `warp_smem`
+// holds p2g_warp_floats(P) floats (16-byte aligned), `stage_base` kStageLanes
+// ints of shared memory.
+template <int ORDER, int LPP>
+__device__ void p2g_item(const P2GArgs& A, int64_t t, int64_t a, int64_t b, float* warp_smem,
+                         int* stage_base)
+{
+    using C = P2GCfg<ORDER, LPP>;
+    using Acc = P2GAcc<ORDER, LPP>;
+    constexpr int K = C::K;
+    const MeshP& mp = A.mp;
+    const TileP& tp = A.tp;
+    const int lane = threadIdx.x & 31;
+    const int run = lane / LPP, h = lane % LPP;
+    float* ring = warp_smem;
+    float* stage = warp_smem + C::STAGE_OFF;
+    float* tile = warp_smem + C::TILE_OFF;
+
+    int ob[3];
+    tile_origin(tp, t, ob);
+    const int U = (int)((b - a + C::RUNS - 1) / C::RUNS);
+    const int64_t my0 = a + (int64_t)run * U;
+    const int cnt = (int)max((int64_t)0, min(my0 + U, b) - my0);
+
+    for (int i = lane; i < 4 * tp.P; i += 32) tile[i] = 0.f;
+    MergePlan<ORDER, LPP> plan;
+    plan.init(tp, lane);
+    const float D = (ORDER >= 2) ? inertial_scaling<ORDER, float>(mp.dx[0]) : 1.f;
+
+    auto slot = [&](int q) { return ring + (q % kRing) * C::RING; };
+    // the 7 copies of a particle record (x0..x2, c0..c2, m) are spread over
+    // the run's lanes: copy j is issued by lane h == j % LPP
+    auto issue = [&](int q) {
+        if (q < cnt) {
+            const int64_t p = my0 + q;
+            float* s = slot(q);
+            float* sx = s + C::RING_X + run * 6;
+            float* sc = s + C::RING_C + run * 12;
+#pragma unroll
+            for (int j = 0; j < 7; ++j) {
+                if (j % LPP != h) continue;
+                if (j < 3) cp_async<8>(sx + 2 * j, A.x + 3 * p + j);
+                else if (j < 6) cp_async<16>(sc + 4 * (j - 3), A.c + 12 * p + 4 * (j - 3));
+                else cp_async<4>(s + C::RING_M + run, A.m + p);
+            }
+        }
+        cp_async_commit();
+    };
+#pragma unroll
+    for (int q = 0; q < kRing - 1; ++q) issue(q);
+
+    Acc acc;
+    acc.zero();
+    int cur = -1, cur_base = 0;
+    int bmin[3] = {1 << 30, 1 << 30, 1 << 30}, bmax[3] = {-1, -1, -1};
+    for (int s = 0; s < U; ++s) {
+        __syncwarp();  // no lane still reads the slot refilled next
+        issue(s + kRing - 1);
+        cp_async_wait<kRing - 1>();
+        if (LPP > 1) __syncwarp();  // a run's copies are visible to all its lanes
+        const bool valid = s < cnt;
+        Spline1D<ORDER, float> sp[3];
+        int lb[3] = {0, 0, 0};
+        bool ok = false;
+        float co[C::F][4], mass = 0.f;
+        if (valid) {
+            const float* sl = slot(s);
+            const double* sx = reinterpret_cast<const double*>(sl + C::RING_X + run * 6);
+            const double xp[3] = {sx[0], sx[1], sx[2]};
+            ok = locate<ORDER>(mp, tp, xp, ob, sp, lb);
+            if (!ok && A.err && h == 0) atomicAdd(A.err, 1);
+            const float* sc = sl + C::RING_C + run * 12;
+            float cp[12];
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                const float4 v = *reinterpret_cast<const float4*>(sc + 4 * q);
+                cp[4 * q] = v.x;
+                cp[4 * q + 1] = v.y;
+                cp[4 * q + 2] = v.z;
+                cp[4 * q + 3] = v.w;
+            }
+            mass = sl[C::RING_M + run];
+            // cp[r * 3 + d] = c_p(r, d)
+#pragma unroll
+            for (int f = 0; f < C::F; ++f) {
+                const int g = h * C::F + f;  // global field
+                if (g == 0) {
+                    co[f][0] = 1.f;
+                    co[f][1] = co[f][2] = co[f][3] = 0.f;
+                } else {
+                    const int d = g - 1;
+                    const float vd = d == 0 ? cp[0] : (d == 1 ? cp[1] : cp[2]);
+                    const float b0 = d == 0 ? cp[3] : (d == 1 ? cp[4] : cp[5]);
+                    const float b1 = d == 0 ? cp[6] : (d == 1 ? cp[7] : cp[8]);
+                    const float b2 = d == 0 ? cp[9] : (d == 1 ? cp[10] : cp[11]);
+                    co[f][0] = vd;
+                    co[f][1] = D * b0;
+                    co[f][2] = D * b1;
+                    co[f][3] = D * b2;
+                }
+            }
+        }
+        const int lbin = ok ? (lb[0] * tp.T[1] + lb[1]) * tp.T[2] + lb[2] : -1;
+        const unsigned fm = __ballot_sync(kFull, ok && cur >= 0 && lbin != cur);
+        if (fm) merge_partials<ORDER, LPP>(fm, acc, cur_base, plan, tile, stage, stage_base, lane);
+        if (ok) {
+            if (lbin != cur) {
+                cur = lbin;
+                cur_base = lb[0] * tp.SI + lb[1] * tp.SJ + lb[2];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    bmin[d] = min(bmin[d], lb[d]);
+                    bmax[d] = max(bmax[d], lb[d]);
+                }
+            }
+            acc.add(sp, mass, co);
+        }
+    }
+    cp_async_wait<0>();
+    const unsigned fm = __ballot_sync(kFull, cur >= 0);
+    if (fm) merge_partials<ORDER, LPP>(fm, acc, cur_base, plan, tile, stage, stage_base, lane);
+    // touched node box, rounded to fixed point and added to HBM
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            bmin[d] = min(bmin[d], __shfl_xor_sync(kFull, bmin[d], o));
+            bmax[d] = max(bmax[d], __shfl_xor_sync(kFull, bmax[d], o));
+        }
+    }
+    if (bmax[0] >= 0) {
+        const int e0 = bmax[0] - bmin[0] + K, e1 = bmax[1] - bmin[1] + K;
+        const int e2 = bmax[2] - bmin[2] + K;
+        const int total = e0 * e1 * e2;
+        for (int e = lane; e < total; e += 32) {
+            const int k = bmin[2] + e % e2;
+            const int j = bmin[1] + (e / e2) % e1;
+            const int i = bmin[0] + e / (e1 * e2);
+            const int idx = i * tp.SI + j * tp.SJ + k;
+            const int gi = node_global(mp, tp, 0, ob[0], i);
+            const int gj = node_global(mp, tp, 1, ob[1], j);
+            const int gk = node_global(mp, tp, 2, ob[2], k);
+#pragma unroll
+            for (int f = 0; f < 4; ++f) {
+                const float v = tile[f * tp.P + idx];
+                if (v != 0.f) {
+                    const long long q = __float2ll_rn(v * (f == 0 ? A.scale_m : A.scale_mu));
+                    unsigned long long* dst = reinterpret_cast<unsigned long long*>(
+                        f == 0 ? A.gm.ptr<long long>(gi, gj, gk, 0)
+                               : A.gmu.ptr<long long>(gi, gj, gk, f - 1));
+                    atomicAdd(dst, (unsigned long long)q);
+                }
+            }
+        }
+    }
+    __syncwarp();
+}
+
+// ---------------------------------------------------------------------------
+// G2P
+// ---------------------------------------------------------------------------
+// One G2P work item by NTHR threads (a warp or a CTA) sharing `tile`
+// (tp.nodes float4).  Threads are numbered tid in [0, NTHR).
+template <int ORDER, int NTHR>
+__device__ void g2p_item(const G2PArgs& A, int64_t t, int64_t a, int64_t b, float4* tile,
+                         int tid)
+{
+    constexpr int K = SplineTraits<ORDER>::K;
+    const MeshP& mp = A.mp;
+    const TileP& tp = A.tp;
+    auto sync = [] {
+        if (NTHR == 32) __syncwarp();
+        else __syncthreads();
+    };
+    int ob[3];
+    tile_origin(tp, t, ob);
+    // bin rows spanned by the item: the first and last particle bound the
+    // slowest tile dimension (keys are i-major within a tile)
+    int i_lo = 0, i_hi = tp.T[0] - 1;
+    {
+        Spline1D<ORDER, float> sp[3];
+        int lb[3];
+        const double xa[3] = {A.x[3 * a], A.x[3 * a + 1], A.x[3 * a + 2]};
+        const double xb[3] = {A.x[3 * (b - 1)], A.x[3 * (b - 1) + 1], A.x[3 * (b - 1) + 2]};
+        const bool oka = locate<ORDER>(mp, tp, xa, ob, sp, lb);
+        const int la = lb[0];
+        const bool okb = locate<ORDER>(mp, tp, xb, ob, sp, lb);
+        if (oka && okb && lb[0] >= la) {
+            i_lo = la;
+            i_hi = lb[0];
+        }
+    }
+    const int plane = tp.NT[1] * tp.NT[2];
+    const int total = (i_hi - i_lo + K) * plane;
+    sync();  // the previous item's threads are done with the tile
+    for (int e = tid; e < total; e += NTHR) {
+        const int k = e % tp.NT[2];
+        const int j = (e / tp.NT[2]) % tp.NT[1];
+        const int i = i_lo + e / plane;
+        const int gi = node_global(mp, tp, 0, ob[0], i);
+        const int gj = node_global(mp, tp, 1, ob[1], j);
+        const int gk = node_global(mp, tp, 2, ob[2], k);
+        const bool inside = (mp.periodic[0] || gi < mp.ext[0]) &&
+                            (mp.periodic[1] || gj < mp.ext[1]) &&
+                            (mp.periodic[2] || gk < mp.ext[2]);
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (inside) {  // through L2: the batched kernel writes u_i in the same launch
+            v.x = __ldcg(A.u.ptr<float>(gi, gj, gk, 0));
+            v.y = __ldcg(A.u.ptr<float>(gi, gj, gk, 1));
+            v.z = __ldcg(A.u.ptr<float>(gi, gj, gk, 2));
+        }
+        tile[(i * tp.NT[1] + j) * tp.NT[2] + k] = v;
+    }
+    sync();
+    // positions are prefetched one particle ahead
+    double xn[3] = {0.0, 0.0, 0.0};
+    if (a + tid < b) {
+        const int64_t p0 = a + tid;
+        xn[0] = A.x[3 * p0];
+        xn[1] = A.x[3 * p0 + 1];
+        xn[2] = A.x[3 * p0 + 2];
+    }
+    for (int64_t p = a + tid; p < b; p += NTHR) {
+        const double xp[3] = {xn[0], xn[1], xn[2]};
+        const int64_t pn = p + NTHR;
+        if (pn < b) {
+            xn[0] = A.x[3 * pn];
+            xn[1] = A.x[3 * pn + 1];
+            xn[2] = A.x[3 * pn + 2];
+        }
+        Spline1D<ORDER, float> sp[3];
+        int lb[3];
+        if (!locate<ORDER>(mp, tp, xp, ob, sp, lb) || lb[0] < i_lo || lb[0] > i_hi) {
+            if (A.err) atomicAdd(A.err, 1);
+            continue;
+        }
+        const int base = (lb[0] * tp.NT[1] + lb[1]) * tp.NT[2] + lb[2];
+        // APIC.hpp:439-461, contracted one dimension at a time:
+        //   u_p      = sum_i wx_i sum_j wy_j sum_k wz_k u_ijk
+        //   B_p(:,q) = sum_ijk w_ijk u_ijk dist_q  (dist_q along x, y or z)
+        float up[3] = {0.f, 0.f, 0.f};
+        float B[3][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+        float wzdz[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) wzdz[k] = sp[2].w[k] * sp[2].d[k];
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            float A0[3] = {0.f, 0.f, 0.f}, A1[3] = {0.f, 0.f, 0.f}, A2[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+            for (int j = 0; j < K; ++j) {
+                const float4* row = tile + base + (i * tp.NT[1] + j) * tp.NT[2];
+                float S0[3] = {0.f, 0.f, 0.f}, S1[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+                for (int k = 0; k < K; ++k) {
+                    const float4 ue = row[k];
+                    const float uk[3] = {ue.x, ue.y, ue.z};
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        S0[d] += sp[2].w[k] * uk[d];
+                        S1[d] += wzdz[k] * uk[d];
+                    }
+                }
+                const float wy = sp[1].w[j], wydy = wy * sp[1].d[j];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    A0[d] += wy * S0[d];
+                    A1[d] += wydy * S0[d];
+                    A2[d] += wy * S1[d];
+                }
+            }
+            const float wx = sp[0].w[i], wxdx = wx * sp[0].d[i];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                up[d] += wx * A0[d];
+                B[d][0] += wxdx * A0[d];
+                B[d][1] += wx * A1[d];
+                B[d][2] += wx * A2[d];
+            }
+        }
+        // c_p(0, d) = u_p(d); c_p(1 + q, d) = B_p(d, q)  (APIC.hpp:464-471)
+        float4* out = reinterpret_cast<float4*>(A.c + 12 * p);
+        out[0] = make_float4(up[0], up[1], up[2], B[0][0]);
+        out[1] = make_float4(B[1][0], B[2][0], B[0][1], B[1][1]);
+        out[2] = make_float4(B[2][1], B[0][2], B[1][2], B[2][2]);
+    }
+}
+
+// host helpers (tiled.cu)
+bool make_tilep(const MeshP& mp, int order, const picasso_bins& bins, TileP* tp, int lpp = 0);
+int device_smem_optin();
+bool packed_x(const PField& x);
+bool packed_m(const PField& m);
+bool packed_c(const PField& c);
+int default_lpp(int order);
+bool valid_lpp(int order, int lpp);
+size_t p2g_warp_bytes(int order, int lpp, int P);
+
+}  // namespace pb

@@ -48,8 +48,14 @@ def test_descriptor_layout_matches_ctypes(tmp_path):
                                                         "tile_stride", "comp_stride"]),
         "picasso_grid_field": (_abi.GridField, ["data", "dtype", "fixed_bits", "stride"]),
         "picasso_bins": (_abi.Bins, ["tile", "num_tiles", "bin_extent", "order", "location",
-                                     "chunk", "tile_offset", "tile_items"]),
+                                     "chunk", "p2g_lanes", "tile_offset", "tile_items"]),
         "picasso_exec": (_abi.Exec, ["stream", "error_count", "bins"]),
+        "picasso_batch_instance": (_abi.BatchInstance, ["spline", "num_particles", "x_p", "m_p",
+                                                        "c_p", "m_i", "mu_i", "u_i",
+                                                        "mass_threshold", "bins",
+                                                        "error_count"]),
+        "picasso_batch_info": (_abi.BatchInfo, ["count", "precision_form", "grid_blocks",
+                                                "smem_bytes", "items", "particles"]),
     }
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "picasso_b200.h"',
              "int main(void) {"]
@@ -164,3 +170,54 @@ def test_sort_workspace_and_key_range():
     big = _spline(n=2048)  # 2048^3 bins do not fit 32-bit keys
     assert lib.picasso_cell_sort_workspace(C.byref(big), 10, tile, C.byref(nbytes)) == \
         _abi.ERR_OUT_OF_RANGE
+
+
+def _batch_instance(f32=True):
+    inst = _abi.BatchInstance()
+    inst.spline = _spline()
+    inst.num_particles = 10
+    pt = _abi.F32 if f32 else _abi.F64
+    gt = _abi.I64_FIXED if f32 else _abi.F64
+    inst.x_p = _pf()
+    inst.m_p = _pf(pt)
+    inst.m_p.tile_stride = 1
+    inst.c_p = _pf(pt)
+    inst.c_p.tile_stride = 12
+    inst.m_i, inst.mu_i, inst.u_i = _gf(gt), _gf(gt), _gf(pt)
+    b = inst.bins
+    for d in range(3):
+        b.tile[d], b.num_tiles[d], b.bin_extent[d] = 4, 2, 8
+    b.order, b.location, b.chunk = 2, 0, 256
+    b.tile_offset, b.tile_items = 16, 16
+    return inst
+
+
+@pytest.mark.parametrize("case", ["count", "null_out", "location", "mixed_forms", "lanes",
+                                  "bins_order", "layout", "mode"])
+def test_batch_create_rejects_invalid_instances_on_host(case):
+    lib = _abi.load_library()
+    insts = (_abi.BatchInstance * 2)(_batch_instance(), _batch_instance())
+    count, mode = 2, _abi.BATCH_FUSED
+    out = C.c_void_p()
+    out_ptr = C.byref(out)
+    if case == "count":
+        count = 0
+    elif case == "null_out":
+        out_ptr = None
+    elif case == "location":
+        insts[1].spline.location = _abi.CELL
+        insts[1].bins.location = _abi.CELL
+    elif case == "mixed_forms":
+        insts[1] = _batch_instance(f32=False)
+    elif case == "lanes":
+        insts[0].spline.order = insts[0].bins.order = 3
+        insts[0].bins.p2g_lanes = 1
+    elif case == "bins_order":
+        insts[0].bins.order = 1
+    elif case == "layout":
+        insts[1].c_p.tile_stride = 3
+    elif case == "mode":
+        mode = 7
+    st = lib.picasso_batch_create(insts, count, mode, out_ptr)
+    assert st == _abi.ERR_INVALID_ARGUMENT
+    assert not out.value

@@ -32,11 +32,11 @@ def _oracle_step(mesh, loc, order, x, m, c):
     return gm, gmu, gu, co
 
 
-def _gpu_step(mesh, loc, order, x, m, c, tile, sort=True):
+def _gpu_step(mesh, loc, order, x, m, c, tile, sort=True, lanes=0):
     xd = _dev(x)
     md, cd = _dev(m, torch.float32), _dev(c, torch.float32)
     sd = create_spline(loc, order, mesh, xd)
-    key, perm, bins = cell_sort(sd, tile)
+    key, perm, bins = cell_sort(sd, tile, p2g_lanes=lanes)
     if sort:
         xd, md, cd = permute_members(perm, xd, md, cd)
         sd = create_spline(loc, order, mesh, xd)
@@ -57,17 +57,23 @@ def _gpu_step(mesh, loc, order, x, m, c, tile, sort=True):
     return acc, u64, c_out, int(err.item())
 
 
+# (particles, order, bins per tile, P2G lanes per particle; 0 = default)
 CASES = [
-    ("uniform", 2, (8, 8, 8)),
-    ("clustered", 2, (8, 8, 8)),
-    ("clustered", 2, (4, 8, 16)),
-    ("uniform", 1, (8, 8, 8)),
-    ("clustered", 3, (8, 8, 8)),   # cubic: tiled G2P, plain P2G
+    ("uniform", 2, (8, 8, 8), 0),
+    ("clustered", 2, (8, 8, 8), 0),
+    ("clustered", 2, (4, 8, 16), 0),
+    ("uniform", 2, (8, 8, 8), 2),
+    ("clustered", 2, (4, 8, 8), 4),
+    ("uniform", 1, (8, 8, 8), 0),
+    ("clustered", 1, (4, 8, 8), 2),
+    ("uniform", 1, (4, 4, 8), 4),
+    ("clustered", 3, (8, 8, 8), 0),
+    ("uniform", 3, (4, 8, 8), 4),
 ]
 
 
-@pytest.mark.parametrize("kind,order,tile", CASES)
-def test_tiled_vs_oracle(cuda, kind, order, tile):
+@pytest.mark.parametrize("kind,order,tile,lanes", CASES)
+def test_tiled_vs_oracle(cuda, kind, order, tile, lanes):
     mesh = periodic_mesh(24, halo=0)
     if kind == "uniform":
         x, m, c = uniform_particles(mesh, 8, seed=51)
@@ -78,7 +84,7 @@ def test_tiled_vs_oracle(cuda, kind, order, tile):
     c = c.astype(np.float32).astype(np.float64)
     loc = FieldLocation.Node
     gm_o, gmu_o, gu_o, c_o = _oracle_step(mesh, loc, order, x, m, c)
-    acc, u64, c_g, nerr = _gpu_step(mesh, loc, order, x, m, c, tile)
+    acc, u64, c_g, nerr = _gpu_step(mesh, loc, order, x, m, c, tile, lanes=lanes)
     assert nerr == 0
     a = acc.double().cpu().numpy() * 2.0 ** -BITS
     assert rel_err(a[..., 0], gm_o) <= TOL
@@ -89,10 +95,12 @@ def test_tiled_vs_oracle(cuda, kind, order, tile):
     assert rel_err(cg[:, 1:], c_o[:, 1:]) <= TOL
 
 
-def test_tiled_is_bit_reproducible(cuda):
+@pytest.mark.parametrize("order,lanes", [(2, 1), (2, 4), (3, 4)])
+def test_tiled_is_bit_reproducible(cuda, order, lanes):
     mesh = periodic_mesh(32, halo=0)
     x, m, c = clustered_particles(mesh, 32 ** 3 * 8, nblob=8, sigma_cells=2.0, frac=0.7, seed=53)
-    runs = [_gpu_step(mesh, FieldLocation.Node, 2, x, m, c, (8, 8, 8)) for _ in range(3)]
+    runs = [_gpu_step(mesh, FieldLocation.Node, order, x, m, c, (8, 8, 8), lanes=lanes)
+            for _ in range(3)]
     for r in runs[1:]:
         assert torch.equal(r[0], runs[0][0])
         assert torch.equal(r[1], runs[0][1])
@@ -124,3 +132,13 @@ def test_unsorted_particles_with_bins_are_flagged(cuda):
     x, m, c = uniform_particles(mesh, 4, seed=55)
     _, _, _, nerr = _gpu_step(mesh, FieldLocation.Node, 2, x, m, c, (8, 8, 8), sort=False)
     assert nerr > 0
+
+
+@pytest.mark.parametrize("order,lanes", [(3, 1), (3, 2), (2, 3)])
+def test_unsupported_p2g_lanes_are_refused(cuda, order, lanes):
+    from picasso_b200._abi import ERR_INVALID_ARGUMENT, PicassoError
+    mesh = periodic_mesh(16, halo=0)
+    x, m, c = uniform_particles(mesh, 2, seed=56)
+    with pytest.raises(PicassoError) as e:
+        _gpu_step(mesh, FieldLocation.Node, order, x, m, c, (8, 8, 8), lanes=lanes)
+    assert e.value.status == ERR_INVALID_ARGUMENT
