@@ -37,6 +37,18 @@
 namespace pb {
 
 constexpr int kPhases = 4;
+// P2G variants: the phased step runs one P2G kernel per variant, each with the
+// registers of that variant alone.  Precision form: (order, lanes per
+// particle); FP64: order.
+constexpr int kVariants = 7;
+constexpr int kVarOrder[kVariants] = {1, 1, 1, 2, 2, 2, 3};
+constexpr int kVarLanes[kVariants] = {1, 2, 4, 1, 2, 4, 4};
+
+__host__ __device__ constexpr int p2g_variant(bool f32, int order, int lpp)
+{
+    return f32 ? (order == 3 ? 6 : (order - 1) * 3 + (lpp == 1 ? 0 : (lpp == 2 ? 1 : 2)))
+               : order - 1;
+}
 constexpr int kNodeItem = 4096;           // nodes per fill / velocity item
 constexpr unsigned kWaitPolls = 1u << 22;  // ~1-2 s of polling before a wait gives up
 
@@ -55,9 +67,10 @@ struct BInst {
 struct BatchDev {
     const BInst* inst;
     const uint32_t* qbegin;  // kPhases * count + 1 queue offsets, phase-major
-    const int32_t* rank;     // instance at rank r within a phase
+    const int32_t* rank;     // kPhases * count: instance at rank r of phase p
     uint32_t* done;          // kPhases * count completion counters
-    uint32_t* head;          // kPhases queue heads (fused mode uses head[0])
+    uint32_t* head;          // queue heads: one per phase launch, then one per P2G
+                             // variant launch (fused mode uses head[0])
     int* status;             // bit 0: a dependency wait ran out
     int count;
 };
@@ -176,13 +189,26 @@ __device__ __forceinline__ const T& stage_args(const T& src, T* dst, int tid)
 }
 
 // Precision-form P2G items are single-warp (NT = 32); FP64 items any NT.
-template <bool F32, int NT>
+// VAR >= 0: every item of this kernel is of P2G variant VAR (inlined body);
+// VAR < 0: any variant (out-of-line bodies).
+template <bool F32, int NT, int VAR>
 __device__ void p2g_batch_item(const BInst& I, uint32_t local, float* smem, int* stage_base,
                                P2GArgs* args, int tid)
 {
     int64_t t, a, b;
     if (!item_range(I.p2g.tp, local, t, a, b)) return;
-    if constexpr (F32) {
+    if constexpr (VAR >= 0) {
+        constexpr int O = F32 ? kVarOrder[VAR] : VAR + 1;
+        if constexpr (F32) {
+            static_assert(NT == 32, "tiled P2G items are single-warp");
+            const P2GArgs& A = stage_args<P2GArgs, NT>(I.p2g, args, tid);
+            p2g_item<O, kVarLanes[VAR]>(A, t, a, b, smem, stage_base);
+        } else {
+            for (int64_t p = a + tid; p < b; p += NT)
+                apic_p2g_particle<O, 3, false, double, double, AccF64>(
+                    I.p2g.mp, p, I.x, I.m, I.c, I.gm, I.gmu, -1, 0.0, 0.0, I.p2g.err);
+        }
+    } else if constexpr (F32) {
         static_assert(!F32 || NT == 32, "tiled P2G items are single-warp");
         const int key = I.order * 8 + I.lpp;
         const P2GArgs& A = stage_args<P2GArgs, NT>(I.p2g, args, tid);
@@ -228,20 +254,25 @@ __device__ void g2p_batch_item(const BInst& I, uint32_t local, float* smem, G2PA
 // Fused and precision-form P2G kernels are single-warp CTAs (items are
 // per-warp); fill and velocity take 256 threads per item, the other phases
 // 128.
-template <bool F32, int PMASK>
+template <bool F32, int PMASK, int VAR = -1>
 struct BatchShape {
     static constexpr int threads = (PMASK == 0xF || (F32 && PMASK == 0x2)) ? 32
                                    : (PMASK == 0x1 || PMASK == 0x4)       ? 256
                                                                           : 128;
-    static constexpr int min_blocks = threads == 32 ? 8 : (!F32 && threads == 128 ? 3 : 4);
+    // a single-variant precision-form P2G kernel gets the occupancy of the
+    // single-call kernel of that variant
+    static constexpr int p2g_lanes = (VAR >= 0 && F32) ? kVarLanes[VAR] : 1;
+    static constexpr int min_blocks =
+        threads == 32 ? (p2g_lanes == 1 ? 8 : (p2g_lanes == 2 ? 12 : 16))
+                      : (!F32 && threads == 128 ? 3 : 4);
 };
 
-template <bool F32, int PMASK>
-__global__ void __launch_bounds__(BatchShape<F32, PMASK>::threads,
-                                  BatchShape<F32, PMASK>::min_blocks)
+template <bool F32, int PMASK, int VAR = -1>
+__global__ void __launch_bounds__(BatchShape<F32, PMASK, VAR>::threads,
+                                  BatchShape<F32, PMASK, VAR>::min_blocks)
 batch_kernel(BatchDev B, uint32_t qlo, uint32_t qhi, int slot)
 {
-    constexpr int NT = BatchShape<F32, PMASK>::threads;
+    constexpr int NT = BatchShape<F32, PMASK, VAR>::threads;
     extern __shared__ __align__(16) float smem[];
     __shared__ int stage_base[kStageLanes];
     __shared__ uint32_t s_item;
@@ -268,7 +299,7 @@ batch_kernel(BatchDev B, uint32_t qlo, uint32_t qhi, int slot)
             else hi = mid - 1;
         }
         const int ph = lo / B.count;
-        const int i = __ldg(B.rank + (lo - ph * B.count));
+        const int i = __ldg(B.rank + lo);
         const uint32_t local = w - __ldg(B.qbegin + lo);
         const BInst& I = B.inst[i];
         bool run = true;
@@ -278,7 +309,8 @@ batch_kernel(BatchDev B, uint32_t qlo, uint32_t qhi, int slot)
             if constexpr ((PMASK & 0x1) != 0)
                 if (ph == 0) fill_item<F32, NT>(I, local, tid);
             if constexpr ((PMASK & 0x2) != 0)
-                if (ph == 1) p2g_batch_item<F32, NT>(I, local, smem, stage_base, &s_p2g, tid);
+                if (ph == 1)
+                    p2g_batch_item<F32, NT, VAR>(I, local, smem, stage_base, &s_p2g, tid);
             if constexpr ((PMASK & 0x4) != 0)
                 if (ph == 2) velocity_item<F32, NT>(I, local, tid);
             if constexpr ((PMASK & 0x8) != 0)
@@ -303,6 +335,10 @@ struct picasso_batch {
     int device = 0;
     int smem[kPhases + 1] = {0, 0, 0, 0, 0};    // per phase, [kPhases] = fused
     int blocks[kPhases + 1] = {0, 0, 0, 0, 0};
+    // phased P2G: one launch per variant over queue slots [var_lo, var_hi)
+    int var_smem[kVariants] = {};
+    int var_blocks[kVariants] = {};
+    uint32_t var_lo[kVariants] = {}, var_hi[kVariants] = {};
     std::vector<uint32_t> qbegin;
     std::vector<picasso_batch_instance> inst;
     int64_t particles = 0;
@@ -317,18 +353,29 @@ namespace {
 
 using pb::BInst;
 
-template <bool F32, int PMASK>
+template <bool F32, int PMASK, int VAR = -1>
 picasso_status configure_kernel(int smem, int items, int* blocks)
 {
-    auto k = batch_kernel<F32, PMASK>;
+    auto k = batch_kernel<F32, PMASK, VAR>;
     PB_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     int per_sm = 0, dev = 0, sms = 0;
     PB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &per_sm, k, BatchShape<F32, PMASK>::threads, smem));
+        &per_sm, k, BatchShape<F32, PMASK, VAR>::threads, smem));
     PB_CUDA_TRY(cudaGetDevice(&dev));
     PB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     if (per_sm < 1) return PICASSO_ERR_UNSUPPORTED;
     *blocks = std::max(1, std::min(per_sm * sms, items));
+    return PICASSO_OK;
+}
+
+// FP64 has variants 0..2 (orders 1..3) only.
+template <bool F32, int VAR>
+picasso_status configure_variant(picasso_batch* b)
+{
+    if constexpr (F32 || VAR < 3) {
+        const int n = (int)(b->var_hi[VAR] - b->var_lo[VAR]);
+        if (n) return configure_kernel<F32, 0x2, VAR>(b->var_smem[VAR], n, &b->var_blocks[VAR]);
+    }
     return PICASSO_OK;
 }
 
@@ -345,7 +392,26 @@ picasso_status configure(picasso_batch* b)
     if ((st = configure_kernel<F32, 0x1>(b->smem[0], items[0], &b->blocks[0]))) return st;
     if ((st = configure_kernel<F32, 0x2>(b->smem[1], items[1], &b->blocks[1]))) return st;
     if ((st = configure_kernel<F32, 0x4>(b->smem[2], items[2], &b->blocks[2]))) return st;
-    return configure_kernel<F32, 0x8>(b->smem[3], items[3], &b->blocks[3]);
+    if ((st = configure_kernel<F32, 0x8>(b->smem[3], items[3], &b->blocks[3]))) return st;
+    if ((st = configure_variant<F32, 0>(b))) return st;
+    if ((st = configure_variant<F32, 1>(b))) return st;
+    if ((st = configure_variant<F32, 2>(b))) return st;
+    if ((st = configure_variant<F32, 3>(b))) return st;
+    if ((st = configure_variant<F32, 4>(b))) return st;
+    if ((st = configure_variant<F32, 5>(b))) return st;
+    return configure_variant<F32, 6>(b);
+}
+
+template <bool F32, int VAR>
+void launch_p2g_variant(const picasso_batch* b, cudaStream_t s)
+{
+    if constexpr (F32 || VAR < 3) {
+        const uint32_t lo = b->var_lo[VAR], hi = b->var_hi[VAR];
+        if (lo == hi) return;
+        batch_kernel<F32, 0x2, VAR>
+            <<<b->var_blocks[VAR], BatchShape<F32, 0x2, VAR>::threads, b->var_smem[VAR], s>>>(
+                b->dev, lo, hi, kPhases + VAR);
+    }
 }
 
 template <bool F32>
@@ -353,6 +419,16 @@ void launch_phase(const picasso_batch* b, int p, cudaStream_t s)
 {
     const uint32_t lo = b->qbegin[p * b->count], hi = b->qbegin[(p + 1) * b->count];
     if (lo == hi) return;
+    if (p == 1) {  // one launch per P2G variant, each with its own queue head
+        launch_p2g_variant<F32, 0>(b, s);
+        launch_p2g_variant<F32, 1>(b, s);
+        launch_p2g_variant<F32, 2>(b, s);
+        launch_p2g_variant<F32, 3>(b, s);
+        launch_p2g_variant<F32, 4>(b, s);
+        launch_p2g_variant<F32, 5>(b, s);
+        launch_p2g_variant<F32, 6>(b, s);
+        return;
+    }
 #define PB_PHASE(P, M)                                                                  \
     batch_kernel<F32, M><<<b->blocks[P], BatchShape<F32, M>::threads, b->smem[P], s>>>(    \
         b->dev, lo, hi, P)
@@ -489,18 +565,38 @@ extern "C" picasso_status picasso_batch_create(const picasso_batch_instance* ins
     b->smem[3] = smem_g2p;
     b->smem[kPhases] = std::max(smem_p2g, smem_g2p);
     b->inst.assign(instances, instances + count);
-    // queue: phase-major, instances by decreasing particle count
-    std::vector<int32_t> rank(count);
-    std::iota(rank.begin(), rank.end(), 0);
-    std::stable_sort(rank.begin(), rank.end(), [&](int a, int c) {
+    // queue: phase-major, instances by decreasing particle count; in the P2G
+    // phase grouped by variant first (one phased launch per variant)
+    std::vector<int> var(count);
+    for (int i = 0; i < count; ++i) var[i] = p2g_variant(f32, hinst[i].order, hinst[i].lpp);
+    std::vector<int32_t> by_size(count);
+    std::iota(by_size.begin(), by_size.end(), 0);
+    std::stable_sort(by_size.begin(), by_size.end(), [&](int a, int c) {
         return instances[a].num_particles > instances[c].num_particles;
     });
+    std::vector<int32_t> by_var(by_size);
+    std::stable_sort(by_var.begin(), by_var.end(), [&](int a, int c) { return var[a] < var[c]; });
+    std::vector<int32_t> rank((size_t)kPhases * count);
+    for (int p = 0; p < kPhases; ++p) {
+        const std::vector<int32_t>& order = p == 1 ? by_var : by_size;
+        std::copy(order.begin(), order.end(), rank.begin() + (size_t)p * count);
+    }
     b->qbegin.assign((size_t)kPhases * count + 1, 0);
     uint64_t q = 0;
     for (int p = 0; p < kPhases; ++p)
         for (int r = 0; r < count; ++r) {
+            const int i = rank[(size_t)p * count + r];
             b->qbegin[(size_t)p * count + r] = (uint32_t)q;
-            q += hinst[rank[r]].nitems[p];
+            if (p == 1 && hinst[i].nitems[p]) {
+                const int v = var[i];
+                if (b->var_lo[v] == b->var_hi[v]) b->var_lo[v] = (uint32_t)q;
+                b->var_hi[v] = (uint32_t)(q + hinst[i].nitems[p]);
+                if (f32)
+                    b->var_smem[v] = std::max(b->var_smem[v],
+                                              (int)p2g_warp_bytes(hinst[i].order, hinst[i].lpp,
+                                                                  hinst[i].p2g.tp.P));
+            }
+            q += hinst[i].nitems[p];
         }
     for (int i = 0; i < count; ++i) b->particles += instances[i].num_particles;
     if (q >= (1ULL << 31)) {
@@ -514,8 +610,8 @@ extern "C" picasso_status picasso_batch_create(const picasso_batch_instance* ins
     const size_t o_inst = 0;
     const size_t o_q = align(o_inst + sizeof(BInst) * count);
     const size_t o_rank = align(o_q + sizeof(uint32_t) * b->qbegin.size());
-    const size_t o_done = align(o_rank + sizeof(int32_t) * count);
-    b->counter_bytes = sizeof(uint32_t) * ((size_t)kPhases * count + kPhases);
+    const size_t o_done = align(o_rank + sizeof(int32_t) * rank.size());
+    b->counter_bytes = sizeof(uint32_t) * ((size_t)kPhases * count + kPhases + kVariants);
     const size_t o_status = align(o_done + b->counter_bytes);
     const size_t bytes = o_status + 256;
     auto fail = [&](cudaError_t e) {
@@ -532,7 +628,7 @@ extern "C" picasso_status picasso_batch_create(const picasso_batch_instance* ins
                         cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemcpy(base + o_q, b->qbegin.data(), sizeof(uint32_t) * b->qbegin.size(),
                         cudaMemcpyHostToDevice)) != cudaSuccess ||
-        (e = cudaMemcpy(base + o_rank, rank.data(), sizeof(int32_t) * count,
+        (e = cudaMemcpy(base + o_rank, rank.data(), sizeof(int32_t) * rank.size(),
                         cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemset(base + o_done, 0, b->counter_bytes)) != cudaSuccess ||
         (e = cudaMemset(base + o_status, 0, 256)) != cudaSuccess)
