@@ -58,8 +58,16 @@ def parse():
                     help="keep the generated particle order (plain kernels)")
     ap.add_argument("--cpu-sample-grid", type=int, default=64)
     ap.add_argument("--json-out", default=None)
-    ap.add_argument("--suite", default="step", choices=["step", "batch"],
-                    help="step: the APIC step on one mesh; batch: many independent instances")
+    ap.add_argument("--suite", default="step", choices=["step", "batch", "advect", "polypic"],
+                    help="step: the APIC step on one mesh (default, includes the advect and "
+                         "polypic legs unless --no-legs); batch: many independent instances; "
+                         "advect / polypic: one leg alone")
+    ap.add_argument("--no-legs", action="store_true",
+                    help="skip the cubic advection and PolyPIC legs of the default run")
+    ap.add_argument("--adv-grid", type=int, default=256)
+    ap.add_argument("--adv-steps", type=int, default=10)
+    ap.add_argument("--adv-tile", type=int, nargs=3, default=[4, 4, 8])
+    ap.add_argument("--pp-grid", type=int, default=128)
     ap.add_argument("--batch-instances", type=int, default=512)
     ap.add_argument("--batch-seed", type=int, default=4)
     ap.add_argument("--batch-forms", default="fp32,fp64")
@@ -406,6 +414,15 @@ def run_ours(args):
     e2e = None
     if not args.no_e2e:
         e2e = run_e2e(s32, x, m32, c32, args, stream, dist, world)
+    legs = {}
+    if world == 1 and not args.no_legs:
+        # free the headline workload first: the legs hold their own particles
+        del s32
+        x = m32 = c32 = m64 = c64 = sd0 = None
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        legs["advect_cubic"] = run_advect(args, peak)
+        legs["polypic"] = run_polypic(args, peak)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_sample(args, 3, 1, os.cpu_count() or 1)
@@ -422,7 +439,7 @@ def run_ours(args):
             "step_roofline": {"bytes_per_particle_model": model_bytes,
                               "achieved_gbs": n * model_bytes / (ms32 * 1e-3) / 1e9,
                               "frac": n * model_bytes / (ms32 * 1e-3) / 1e9 / peak["hbm_gbs"]},
-            "kernels": k32, "gpu_launches": s32.launches_per_step * args.steps,
+            "kernels": k32, "gpu_launches": 4 * args.steps,
             "clocks": clocks}
     if "fp64" in out:
         ms64, per64, rf64, k64 = out["fp64"]
@@ -437,6 +454,7 @@ def run_ours(args):
         line["e2e"] = e2e
     if cpu:
         line["cpu_baseline"] = cpu
+    line.update(legs)
     if rank == 0:
         print(json.dumps(line))
         if args.json_out:
@@ -445,6 +463,208 @@ def run_ours(args):
     if dist:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# advection leg: cubic APIC, P2G -> grid update -> G2P + x += dt v -> re-sort
+# ---------------------------------------------------------------------------
+def run_advect(args, peak):
+    """256^3 periodic grid, 8 ppc uniform, cubic B-spline, dt = 0.1 dx: every
+    step zeroes the grid, P2G, velocity update, G2P fused with the position
+    update, then re-sorts the particles by cell and permutes every member.
+    FP64 plain form (the reference's arithmetic) and FP32 precision form
+    (tiled kernels); both forms start from the same particles."""
+    import torch
+
+    import picasso_b200 as pb
+    from picasso_b200 import workloads
+
+    g = args.adv_grid
+    mesh = pb.UniformMesh([0, 0, 0, 1, 1, 1], cell_size=1.0 / g, periodic=(True,) * 3)
+    loc = pb.FieldLocation.Node
+    desc = mesh.descriptor(loc)
+    ext = mesh.extent(loc)
+    dt = 0.1 / g
+    seed = 1001
+    res = {"workload": "cubic APIC, %d^3 periodic, 8 ppc uniform, dt = 0.1 dx, per step: "
+                       "fill, P2G, velocity, G2P + advection, cell re-sort + permute" % g,
+           "steps": args.adv_steps, "tile": list(args.adv_tile)}
+    names = ["sort", "permute", "fill", "p2g", "velocity", "g2p_advect"]
+    for form in ("fp64", "fp32"):
+        f32 = form == "fp32"
+        x = workloads.positions("uniform", g, 8, seed)
+        m, c = workloads.particle_state(x.shape[0], seed,
+                                        dtype=torch.float32 if f32 else torch.float64)
+        c = c.contiguous()
+        n = x.shape[0]
+        if f32:
+            acc = torch.zeros(ext + (4,), dtype=torch.int64, device="cuda")
+            gm = pb.FixedGrid(acc[..., 0], FIXED_BITS)
+            gmu = pb.FixedGrid(acc[..., 1:], FIXED_BITS)
+            fill = pb.FixedGrid(acc, FIXED_BITS)
+            u = torch.zeros(ext + (3,), dtype=torch.float32, device="cuda")
+        else:
+            acc = torch.zeros(ext + (4,), dtype=torch.float64, device="cuda")
+            gm, gmu, fill = acc[..., 0], acc[..., 1:], acc
+            u = torch.zeros(ext + (3,), dtype=torch.float64, device="cuda")
+        state = {"x": x, "m": m, "c": c}
+
+        def step(ev=None):
+            def mark(i):
+                if ev is not None:
+                    ev[i].record()
+            mark(0)
+            sd0 = pb.create_spline(loc, 3, mesh, state["x"])
+            _, perm, bins = pb.cell_sort(sd0, tuple(args.adv_tile), chunk=2048,
+                                         p2g_lanes=4 if f32 else 0)
+            mark(1)
+            state["x"], state["m"], state["c"] = pb.permute_members(
+                perm, state["x"], state["m"], state["c"])
+            mark(2)
+            sd = pb.create_spline(loc, 3, mesh, state["x"])
+            pb.grid_fill(desc, fill, 0.0, ncomp=4)
+            mark(3)
+            pb.APIC.p2g(state["m"], state["c"], gm, gmu, sd, bins=bins)
+            mark(4)
+            pb.grid_velocity(desc, gm, gmu, u, 1e-12)
+            mark(5)
+            pb.APIC.g2p_advect(u, state["c"], sd, dt, bins=bins)
+            mark(6)
+
+        step()
+        torch.cuda.synchronize()
+        ev = [[torch.cuda.Event(enable_timing=True) for _ in range(7)]
+              for _ in range(args.adv_steps)]
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record()
+        for k in range(args.adv_steps):
+            step(ev[k])
+        t1.record()
+        torch.cuda.synchronize()
+        ms = t0.elapsed_time(t1) / args.adv_steps
+        per = {nm: sum(ev[k][q].elapsed_time(ev[k][q + 1]) for k in range(args.adv_steps))
+               / args.adv_steps for q, nm in enumerate(names)}
+        xs = state["x"]
+        res[form] = {"ms_per_step": ms, "particles_per_s": n / (ms * 1e-3),
+                     "transfer_ms": per["fill"] + per["p2g"] + per["velocity"]
+                     + per["g2p_advect"], "kernels_ms": per,
+                     "positions_in_box": bool(float(xs.min()) >= 0.0 and float(xs.max()) < 1.0)}
+        del state, x, m, c, acc, u
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+    res["speedup_fp32_vs_fp64"] = res["fp64"]["ms_per_step"] / res["fp32"]["ms_per_step"]
+    return res
+
+
+# ---------------------------------------------------------------------------
+# PolyPIC leg: 128^3, 8 ppc, quadratic (27 modes) and linear (8 modes)
+# ---------------------------------------------------------------------------
+def run_polypic(args, peak):
+    """128^3 periodic grid, 8 ppc uniform, mode 0 ~ N(0, 1), other modes
+    ~ N(0, 0.05), m ~ U[0.5, 1.5]; step = fill, PolyPIC P2G (dt = 0.1 dx),
+    velocity update, PolyPIC G2P; particles cell-sorted once.  FP64 and FP32
+    forms; per-mode error of the FP32 form against the FP64 result."""
+    import torch
+
+    import picasso_b200 as pb
+    from picasso_b200 import workloads
+
+    g = args.pp_grid
+    mesh = pb.UniformMesh([0, 0, 0, 1, 1, 1], cell_size=1.0 / g, periodic=(True,) * 3)
+    loc = pb.FieldLocation.Node
+    desc = mesh.descriptor(loc)
+    ext = mesh.extent(loc)
+    seed = 1003
+    x = workloads.positions("uniform", g, 8, seed)
+    n = x.shape[0]
+    m64, _ = workloads.particle_state(n, seed)
+    res = {"workload": "PolyPIC, %d^3 periodic, 8 ppc uniform, cell-sorted, per step: fill, "
+                       "P2G, velocity, G2P" % g, "particles": n}
+    for order, nm in ((2, 27), (1, 8)):
+        sd0 = pb.create_spline(loc, order, mesh, x)
+        _, perm, _ = pb.cell_sort(sd0, (4, 8, 8))
+        modes = workloads.polypic_modes(n, nm, seed)
+        xs, ms, us = pb.permute_members(perm, x, m64, modes)
+        sd = pb.create_spline(loc, order, mesh, xs)
+        out = {}
+        finals = {}
+        for form in ("fp64", "fp32"):
+            f32 = form == "fp32"
+            mm = ms.float() if f32 else ms
+            c0 = us.float() if f32 else us
+            c = c0.clone()
+            if f32:
+                acc = torch.zeros(ext + (4,), dtype=torch.int64, device="cuda")
+                gm = pb.FixedGrid(acc[..., 0], FIXED_BITS)
+                gmu = pb.FixedGrid(acc[..., 1:], FIXED_BITS)
+                fill = pb.FixedGrid(acc, FIXED_BITS)
+                u = torch.zeros(ext + (3,), dtype=torch.float32, device="cuda")
+            else:
+                acc = torch.zeros(ext + (4,), dtype=torch.float64, device="cuda")
+                gm, gmu, fill = acc[..., 0], acc[..., 1:], acc
+                u = torch.zeros(ext + (3,), dtype=torch.float64, device="cuda")
+
+            def step(ev=None):
+                if ev is not None:
+                    ev[0].record()
+                pb.grid_fill(desc, fill, 0.0, ncomp=4)
+                pb.PolyPIC.p2g(mm, c, c, gmu, gm, 0.1 / g, sd)
+                if ev is not None:
+                    ev[1].record()
+                pb.grid_velocity(desc, gm, gmu, u, 1e-12)
+                if ev is not None:
+                    ev[2].record()
+                pb.PolyPIC.g2p(u, c, sd)
+                if ev is not None:
+                    ev[3].record()
+
+            c.copy_(c0)
+            step()  # the error comparison uses this first step
+            torch.cuda.synchronize()
+            finals[form] = c.double().clone()
+            for _ in range(max(args.warmup - 1, 0)):
+                step()
+            torch.cuda.synchronize()
+            t0 = torch.cuda.Event(enable_timing=True)
+            t1 = torch.cuda.Event(enable_timing=True)
+            evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)]
+                   for _ in range(args.steps)]
+            t0.record()
+            for k in range(args.steps):
+                step(evs[k])
+            t1.record()
+            torch.cuda.synchronize()
+            msp = t0.elapsed_time(t1) / args.steps
+            kms = {nm: sum(e[q].elapsed_time(e[q + 1]) for e in evs) / args.steps
+                   for q, nm in enumerate(["fill_p2g", "velocity", "g2p"])}
+            out[form] = {"ms_per_step": msp, "particles_per_s": n / (msp * 1e-3),
+                         "kernels_ms": kms}
+            del acc, u, c
+        ref = finals["fp64"]
+        err = (finals["fp32"] - ref).abs().amax(dim=(0, 2)) / ref.abs().amax(dim=(0, 2))
+        out["fp32_per_mode_rel_err_max"] = float(err.max())
+        out["fp32_per_mode_rel_err"] = [float(e) for e in err]
+        out["speedup_fp32_vs_fp64"] = out["fp64"]["ms_per_step"] / out["fp32"]["ms_per_step"]
+        res["quadratic_27" if order == 2 else "linear_8"] = out
+        del xs, ms, us, modes, perm, sd, sd0, finals
+        torch.cuda.empty_cache()
+    return res
+
+
+def run_leg_alone(args):
+    import torch
+    torch.cuda.set_device(0)
+    peak = peaks()
+    clk = Clocks(0)
+    clk.start()
+    r = run_advect(args, peak) if args.suite == "advect" else run_polypic(args, peak)
+    r["clocks"] = clk.stop()
+    line = json.dumps({"suite": args.suite, **r})
+    print(line)
+    if args.json_out:
+        with open(args.json_out, "w") as f:
+            f.write(line + "\n")
 
 
 def run_e2e(step, x, m32, c32, args, stream, dist, world):
@@ -664,6 +884,8 @@ def main():
         run_reference(args)
     elif args.suite == "batch":
         run_batch(args)
+    elif args.suite in ("advect", "polypic"):
+        run_leg_alone(args)
     else:
         run_ours(args)
 

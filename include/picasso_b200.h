@@ -255,6 +255,20 @@ PICASSO_API picasso_status picasso_advect(const picasso_mesh* mesh, int64_t num_
                               double dt, picasso_particle_field x_p,
                               picasso_particle_field c_p, const picasso_exec* exec);
 
+/* picasso_apic_g2p (collocated, 3 components) followed by picasso_advect on
+ * the same particles, in one pass: each particle's new velocity is written
+ * to c_p and its position moved by dt times that velocity (as stored in
+ * c_p's type) before the next particle.  Same results, bit for bit, as the
+ * two calls; saves re-reading x_p and c_p.  The G2P half replaces
+ * APIC.hpp:407-472; the position update is application code in the
+ * reference (doc/basic/explict_nearly_incompressible_flow.md). */
+PICASSO_API picasso_status picasso_apic_g2p_advect(const picasso_spline* sd,
+                                                   int64_t num_particles,
+                                                   picasso_particle_field x_p,
+                                                   picasso_grid_field u_i,
+                                                   picasso_particle_field c_p, double dt,
+                                                   const picasso_exec* exec);
+
 /* ------------------------------------------------------------------------ */
 /* Particle cell-sort                                                       */
 /* ------------------------------------------------------------------------ */

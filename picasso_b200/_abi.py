@@ -105,6 +105,9 @@ SIGNATURES = [
       C.POINTER(Exec)]),
     ("picasso_advect", C.c_int,
      [C.POINTER(Mesh), C.c_int64, C.c_double, ParticleField, ParticleField, C.POINTER(Exec)]),
+    ("picasso_apic_g2p_advect", C.c_int,
+     [C.POINTER(Spline), C.c_int64, ParticleField, GridField, ParticleField, C.c_double,
+      C.POINTER(Exec)]),
     ("picasso_cell_sort_workspace", C.c_int,
      [C.POINTER(Spline), C.c_int64, C.POINTER(C.c_int32), C.POINTER(C.c_int64)]),
     ("picasso_cell_sort", C.c_int,

@@ -314,6 +314,18 @@ class APIC:
                                       particle_field(sd.x), grid_field(u_i), particle_field(c_p),
                                       C.byref(ex.desc)), "APIC::g2p")
 
+    @staticmethod
+    def g2p_advect(u_i, c_p, sd, dt, stream=None, error_count=None, bins=None):
+        """APIC::g2p followed by the position update x_p += dt * c_p(0, :)
+        (FP64, periodic wrap) in one pass; collocated, 3 components.  The
+        spline's positions sd.x are updated in place."""
+        _check_grid_extent(u_i, sd.desc.mesh)
+        ex = _exec(stream, error_count, bins)
+        check(_lib().picasso_apic_g2p_advect(C.byref(sd.desc), sd.num_particles,
+                                             particle_field(sd.x), grid_field(u_i),
+                                             particle_field(c_p), float(dt), C.byref(ex.desc)),
+              "APIC::g2p_advect")
+
 
 class PolyPIC:
     """Picasso::PolyPIC transfers (linear 8 modes; quadratic 27 modes)."""

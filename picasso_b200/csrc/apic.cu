@@ -21,13 +21,14 @@ apic_p2g_kernel(MeshP mp, int64_t n, PField x, PField m, PField c, GField gm, GF
                                                        scale_mu, err);
 }
 
-template <int ORDER, int NC, bool STAG, class GT, class PT, class R>
+template <int ORDER, int NC, bool STAG, class GT, class PT, class R, bool ADV>
 __global__ void __launch_bounds__(256)
-apic_g2p_kernel(MeshP mp, int64_t n, PField x, GField u, PField c, int stag, int* err)
+apic_g2p_kernel(MeshP mp, int64_t n, PField x, GField u, PField c, int stag, int* err, Advect adv)
 {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride)
-        apic_g2p_particle<ORDER, NC, STAG, GT, PT, R>(mp, p, x, u, c, stag, err);
+        apic_g2p_particle<ORDER, NC, STAG, GT, PT, R, false, ADV>(mp, p, x, u, c, stag, err,
+                                                                   &adv);
 }
 
 // ---------------------------------------------------------------------------
@@ -54,18 +55,31 @@ static void launch_p2g(Form form, const MeshP& mp, int64_t n, const PField& x, c
     }
 }
 
+// adv != nullptr (collocated, 3 components only): G2P then the position update.
 template <int ORDER, int NC, bool STAG>
 static void launch_g2p(bool f32, const MeshP& mp, int64_t n, const PField& x, const GField& u,
-                       const PField& c, int stag, int* err, cudaStream_t st)
+                       const PField& c, int stag, int* err, const Advect* adv, cudaStream_t st)
 {
     const int threads = 256;
     const unsigned blocks = grid_for(n, threads);
+    const Advect a = adv ? *adv : Advect{};
+    if constexpr (NC == 3 && !STAG) {
+        if (adv) {
+            if (f32)
+                apic_g2p_kernel<ORDER, NC, STAG, float, float, float, true>
+                    <<<blocks, threads, 0, st>>>(mp, n, x, u, c, stag, err, a);
+            else
+                apic_g2p_kernel<ORDER, NC, STAG, double, double, double, true>
+                    <<<blocks, threads, 0, st>>>(mp, n, x, u, c, stag, err, a);
+            return;
+        }
+    }
     if (f32)
-        apic_g2p_kernel<ORDER, NC, STAG, float, float, float><<<blocks, threads, 0, st>>>(
-            mp, n, x, u, c, stag, err);
+        apic_g2p_kernel<ORDER, NC, STAG, float, float, float, false><<<blocks, threads, 0, st>>>(
+            mp, n, x, u, c, stag, err, a);
     else
-        apic_g2p_kernel<ORDER, NC, STAG, double, double, double><<<blocks, threads, 0, st>>>(
-            mp, n, x, u, c, stag, err);
+        apic_g2p_kernel<ORDER, NC, STAG, double, double, double, false>
+            <<<blocks, threads, 0, st>>>(mp, n, x, u, c, stag, err, a);
 }
 
 #define PB_ORDER_SWITCH(order, ...)               \
@@ -93,16 +107,16 @@ picasso_status apic_p2g_plain(const MeshP& mp, int order, int stag, int ncomp, F
 
 picasso_status apic_g2p_plain(const MeshP& mp, int order, int stag, int ncomp, bool f32,
                               int64_t n, const PField& x, const GField& u, const PField& c,
-                              int* err, cudaStream_t st)
+                              int* err, const Advect* adv, cudaStream_t st)
 {
     if (stag >= 0) {
-        PB_ORDER_SWITCH(order, launch_g2p<O_, 3, true>(f32, mp, n, x, u, c, stag, err, st));
+        PB_ORDER_SWITCH(order, launch_g2p<O_, 3, true>(f32, mp, n, x, u, c, stag, err, nullptr, st));
     } else if (ncomp == 1) {
-        PB_ORDER_SWITCH(order, launch_g2p<O_, 1, false>(f32, mp, n, x, u, c, -1, err, st));
+        PB_ORDER_SWITCH(order, launch_g2p<O_, 1, false>(f32, mp, n, x, u, c, -1, err, nullptr, st));
     } else if (ncomp == 2) {
-        PB_ORDER_SWITCH(order, launch_g2p<O_, 2, false>(f32, mp, n, x, u, c, -1, err, st));
+        PB_ORDER_SWITCH(order, launch_g2p<O_, 2, false>(f32, mp, n, x, u, c, -1, err, nullptr, st));
     } else {
-        PB_ORDER_SWITCH(order, launch_g2p<O_, 3, false>(f32, mp, n, x, u, c, -1, err, st));
+        PB_ORDER_SWITCH(order, launch_g2p<O_, 3, false>(f32, mp, n, x, u, c, -1, err, adv, st));
     }
     return check_launch();
 }
@@ -114,7 +128,8 @@ picasso_status apic_p2g_tiled(const MeshP& mp, int order, int ncomp, Form form, 
                               cudaStream_t st, bool* handled);
 picasso_status apic_g2p_tiled(const MeshP& mp, int order, int ncomp, bool f32, int64_t n,
                               const PField& x, const GField& u, const PField& c,
-                              const picasso_bins& bins, int* err, cudaStream_t st, bool* handled);
+                              const picasso_bins& bins, int* err, const Advect* adv,
+                              cudaStream_t st, bool* handled);
 
 }  // namespace pb
 
@@ -162,10 +177,11 @@ extern "C" picasso_status picasso_apic_p2g(const picasso_spline* sd, int64_t num
                           err, s);
 }
 
-extern "C" picasso_status picasso_apic_g2p(const picasso_spline* sd, int64_t num_particles,
-                                           int32_t ncomp, picasso_particle_field x_p,
-                                           picasso_grid_field u_i, picasso_particle_field c_p,
-                                           const picasso_exec* exec)
+// G2P, and with dt != nullptr the position update x += dt u_p after it.
+static picasso_status apic_g2p_entry(const picasso_spline* sd, int64_t num_particles,
+                                     int32_t ncomp, picasso_particle_field x_p,
+                                     picasso_grid_field u_i, picasso_particle_field c_p,
+                                     const double* dt, const picasso_exec* exec)
 {
     MeshP mp;
     picasso_status st = make_mesh(sd, &mp);
@@ -173,6 +189,7 @@ extern "C" picasso_status picasso_apic_g2p(const picasso_spline* sd, int64_t num
     if (num_particles < 0) return PICASSO_ERR_INVALID_ARGUMENT;
     const int stag = staggered_dim(sd->location);
     if (stag >= 0 ? ncomp != 3 : (ncomp < 1 || ncomp > 3)) return PICASSO_ERR_INVALID_ARGUMENT;
+    if (dt && (stag >= 0 || ncomp != 3)) return PICASSO_ERR_INVALID_ARGUMENT;
     if ((st = validate_pfield(x_p, PICASSO_F64))) return st;
     if ((st = validate_gfield(u_i, PICASSO_F64, PICASSO_F32))) return st;
     if ((st = validate_pfield(c_p, u_i.dtype))) return st;
@@ -182,15 +199,36 @@ extern "C" picasso_status picasso_apic_g2p(const picasso_spline* sd, int64_t num
     int* err = exec ? exec->error_count : nullptr;
     PField x = make_pfield(x_p), c = make_pfield(c_p);
     GField u = make_gfield(u_i);
+    Advect adv;
+    if (dt) adv = make_advect(sd->mesh, *dt);
+    const Advect* ap = dt ? &adv : nullptr;
     if (exec && exec->bins) {
         if (exec->bins->order != sd->order || exec->bins->location != sd->location)
             return PICASSO_ERR_INVALID_ARGUMENT;
         bool handled = false;
         if (stag < 0) {
             st = apic_g2p_tiled(mp, sd->order, ncomp, f32, num_particles, x, u, c, *exec->bins,
-                                err, s, &handled);
+                                err, ap, s, &handled);
             if (st || handled) return st;
         }
     }
-    return apic_g2p_plain(mp, sd->order, stag, ncomp, f32, num_particles, x, u, c, err, s);
+    return apic_g2p_plain(mp, sd->order, stag, ncomp, f32, num_particles, x, u, c, err, ap, s);
+}
+
+extern "C" picasso_status picasso_apic_g2p(const picasso_spline* sd, int64_t num_particles,
+                                           int32_t ncomp, picasso_particle_field x_p,
+                                           picasso_grid_field u_i, picasso_particle_field c_p,
+                                           const picasso_exec* exec)
+{
+    return apic_g2p_entry(sd, num_particles, ncomp, x_p, u_i, c_p, nullptr, exec);
+}
+
+extern "C" picasso_status picasso_apic_g2p_advect(const picasso_spline* sd,
+                                                  int64_t num_particles,
+                                                  picasso_particle_field x_p,
+                                                  picasso_grid_field u_i,
+                                                  picasso_particle_field c_p, double dt,
+                                                  const picasso_exec* exec)
+{
+    return apic_g2p_entry(sd, num_particles, 3, x_p, u_i, c_p, &dt, exec);
 }

@@ -46,24 +46,13 @@ static void launch_velocity(int ncomp, Box b, GField gm, GField gmu, GField gu, 
 }
 
 template <class CT>
-__global__ void advect_kernel(int64_t n, PField x, PField c, double dt, int3 periodic,
-                              double3 lo, double3 len)
+__global__ void advect_kernel(int64_t n, PField x, PField c, Advect a)
 {
     for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
          p += (int64_t)gridDim.x * blockDim.x) {
-        const int per[3] = {periodic.x, periodic.y, periodic.z};
-        const double l0[3] = {lo.x, lo.y, lo.z};
-        const double ln[3] = {len.x, len.y, len.z};
 #pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            // rounded step by step, as the FP64 update x + (dt * v)
-            double xn = __dadd_rn(x.get<double>(p, d), __dmul_rn(dt, (double)c.get<CT>(p, d)));
-            if (per[d]) {
-                if (xn < l0[d]) xn += ln[d];
-                else if (xn >= l0[d] + ln[d]) xn -= ln[d];
-            }
-            x.set<double>(p, d, xn);
-        }
+        for (int d = 0; d < 3; ++d)
+            x.set<double>(p, d, advect_coord(a, d, x.get<double>(p, d), (double)c.get<CT>(p, d)));
     }
 }
 
@@ -144,21 +133,12 @@ extern "C" picasso_status picasso_advect(const picasso_mesh* mesh, int64_t num_p
     if ((st = validate_pfield(c_p, PICASSO_F64, PICASSO_F32))) return st;
     if (num_particles == 0) return PICASSO_OK;
     PField x = make_pfield(x_p), c = make_pfield(c_p);
-    int3 per = make_int3(mesh->periodic[0] != 0, mesh->periodic[1] != 0, mesh->periodic[2] != 0);
-    double l[3], n[3];
-    for (int d = 0; d < 3; ++d) {
-        l[d] = mesh->low_corner[d] + mesh->own_begin[d] * mesh->cell_size[d];
-        n[d] = mesh->own_extent[d] * mesh->cell_size[d];
-    }
+    const Advect a = make_advect(*mesh, dt);
     cudaStream_t s = stream_of(exec);
     const unsigned blocks = grid_for(num_particles, 256);
     if (c_p.dtype == PICASSO_F64)
-        advect_kernel<double><<<blocks, 256, 0, s>>>(num_particles, x, c, dt, per,
-                                                     make_double3(l[0], l[1], l[2]),
-                                                     make_double3(n[0], n[1], n[2]));
+        advect_kernel<double><<<blocks, 256, 0, s>>>(num_particles, x, c, a);
     else
-        advect_kernel<float><<<blocks, 256, 0, s>>>(num_particles, x, c, dt, per,
-                                                    make_double3(l[0], l[1], l[2]),
-                                                    make_double3(n[0], n[1], n[2]));
+        advect_kernel<float><<<blocks, 256, 0, s>>>(num_particles, x, c, a);
     return check_launch();
 }

@@ -60,4 +60,36 @@ __device__ __forceinline__ void velocity_node(const GField& gm, const GField& gm
     }
 }
 
+// Position update x += dt v with periodic wrap into the owned box, FP64,
+// rounded step by step as x + (dt * v) (no FMA, so every path that advects
+// gives the same bits).
+struct Advect {
+    double dt;
+    int periodic[3];
+    double lo[3];   // coordinate of the owned box's low face
+    double len[3];  // owned box length
+};
+
+inline Advect make_advect(const picasso_mesh& m, double dt)
+{
+    Advect a;
+    a.dt = dt;
+    for (int d = 0; d < 3; ++d) {
+        a.periodic[d] = m.periodic[d] != 0;
+        a.lo[d] = m.low_corner[d] + m.own_begin[d] * m.cell_size[d];
+        a.len[d] = m.own_extent[d] * m.cell_size[d];
+    }
+    return a;
+}
+
+__device__ __forceinline__ double advect_coord(const Advect& a, int d, double x, double v)
+{
+    double xn = __dadd_rn(x, __dmul_rn(a.dt, v));
+    if (a.periodic[d]) {
+        if (xn < a.lo[d]) xn += a.len[d];
+        else if (xn >= a.lo[d] + a.len[d]) xn -= a.len[d];
+    }
+    return xn;
+}
+
 }  // namespace pb

@@ -5,6 +5,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "gridops.cuh"
 #include "transfer.cuh"
 
 namespace pb {
@@ -129,10 +130,13 @@ __device__ __forceinline__ void apic_p2g_particle(const MeshP& mp, int64_t p, co
 // ---------------------------------------------------------------------------
 // GT: grid storage type of u_i; PT: particle storage type of c_p.
 // CG: load u_i through L2 only (for grids written earlier in the same launch).
-template <int ORDER, int NC, bool STAG, class GT, class PT, class R, bool CG = false>
+// ADV (collocated, 3 components): then moves the particle, x += dt u_p with
+// the stored (PT-rounded) u_p, exactly as picasso_advect would afterwards.
+template <int ORDER, int NC, bool STAG, class GT, class PT, class R, bool CG = false,
+          bool ADV = false>
 __device__ __forceinline__ void apic_g2p_particle(const MeshP& mp, int64_t p, const PField& x,
                                                   const GField& u, const PField& c, int stag,
-                                                  int* err)
+                                                  int* err, const Advect* adv = nullptr)
 {
     constexpr int K = SplineTraits<ORDER>::K;
     constexpr int NCO = STAG ? 3 : NC;
@@ -197,6 +201,12 @@ __device__ __forceinline__ void apic_g2p_particle(const MeshP& mp, int64_t p, co
         c.set<PT>(p, 0 * NCO + d, (PT)up[d]);
 #pragma unroll
         for (int a = 0; a < 3; ++a) c.set<PT>(p, (1 + a) * NCO + d, (PT)B[d][a]);
+    }
+    if constexpr (ADV) {
+        static_assert(!STAG && NC == 3, "advection needs the 3-component collocated velocity");
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+            x.set<double>(p, d, advect_coord(*adv, d, x.get<double>(p, d), (double)(PT)up[d]));
     }
 }
 

@@ -25,6 +25,24 @@ __host__ __device__ __forceinline__ constexpr int mode_deg(int r, int d)
                   (2 * r)) & 3ull);
 }
 
+// Inverse of mode_deg: the mode with degrees (a, b, c) (all below D).
+__host__ __device__ __forceinline__ constexpr int mode_of(int a, int b, int c)
+{
+    int r = 0;
+    while (!(mode_deg(r, 0) == a && mode_deg(r, 1) == b && mode_deg(r, 2) == c)) ++r;
+    return r;
+}
+
+// a[i] for a register array and a run-time i (a select chain, no local memory).
+template <int K, class T>
+__device__ __forceinline__ T pick(const T (&a)[K], int i)
+{
+    T v = a[0];
+#pragma unroll
+    for (int q = 1; q < K; ++q) v = (i == q) ? a[q] : v;
+    return v;
+}
+
 template <class R>
 __device__ __forceinline__ R quad_alpha(R p, R h)
 {
@@ -65,7 +83,6 @@ polypic_p2g_kernel(MeshP mp, int64_t n, PField x, PField m, PField u, PField c, 
                    GField gm, R dt, int col, R scale_mu, R scale_m, int* err)
 {
     constexpr int K = SplineTraits<ORDER>::K;
-    constexpr int NM = (ORDER == 1) ? 8 : 27;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
         Spline1D<ORDER, R> sp[3];
@@ -100,58 +117,76 @@ polypic_p2g_kernel(MeshP mp, int64_t n, PField x, PField m, PField u, PField c, 
         }
         // modes of the transferred field: all NC columns, or column `col`
         constexpr int NCU = STAG ? 1 : NC;
+        constexpr int D = ORDER + 1;  // modes per dimension: degrees 0 .. ORDER
         const int ncp = STAG ? (col >= 0 ? NC : 1) : NC;
-        R cp[NM][NCU];
+        // The components are transferred in passes of CB (27 FP64 modes: one
+        // at a time, so that a pass holds 27 mode values rather than 81 in
+        // registers).
+        // The basis sum sum_r c_r b_r(xi) is contracted one dimension at a
+        // time: sum_a f0_a sum_b f1_b sum_c f2_c c_(abc).
+        constexpr int CB = (sizeof(R) == 8 && ORDER == 2) ? 1 : NCU;
+#pragma unroll 1
+        for (int d0 = 0; d0 < NCU; d0 += CB) {
+            R cp[D][D][D][CB];
 #pragma unroll
-        for (int r = 0; r < NM; ++r)
+            for (int a = 0; a < D; ++a)
 #pragma unroll
-            for (int d = 0; d < NCU; ++d)
-                cp[r][d] = (R)c.get<PT>(p, r * ncp + (STAG ? col : d));
+                for (int b = 0; b < D; ++b)
 #pragma unroll
-        for (int i = 0; i < K; ++i)
+                    for (int cc = 0; cc < D; ++cc)
 #pragma unroll
-            for (int j = 0; j < K; ++j)
+                        for (int e = 0; e < CB; ++e)
+                            cp[a][b][cc][e] = (R)c.get<PT>(
+                                p, mode_of(a, b, cc) * ncp + (STAG ? col : d0 + e));
+            // 27 FP64 modes: i-planes one after the other (not unrolled: bounds
+            // the live range of the 9-node plane bodies, which would spill)
+#pragma unroll(sizeof(R) == 8 && ORDER == 2 ? 1 : K)
+            for (int i = 0; i < K; ++i) {
+                const R wxi = pick<K>(sp[0].w, i), dxi = pick<K>(sp[0].d, i);
+                const int gi = pick<K>(idx[0], i);
 #pragma unroll
-                for (int k = 0; k < K; ++k) {
-                    const R wm = mass * sp[0].w[i] * sp[1].w[j] * sp[2].w[k];
-                    const R dist[3] = {sp[0].d[i], sp[1].d[j], sp[2].d[k]};
-                    R map[3];
+                for (int j = 0; j < K; ++j)
 #pragma unroll
-                    for (int a = 0; a < 3; ++a) {
-                        R s = R(0);
+                    for (int k = 0; k < K; ++k) {
+                        const R wm = mass * wxi * sp[1].w[j] * sp[2].w[k];
+                        const R dist[3] = {dxi, sp[1].d[j], sp[2].d[k]};
+                        // backtracked distance xi = A^-1 d (PolyPIC.hpp:90-106)
+                        R map[3];
 #pragma unroll
-                        for (int b = 0; b < 3; ++b) s += ai[3 * a + b] * dist[b];
-                        map[a] = s;
+                        for (int q = 0; q < 3; ++q) {
+                            R t = R(0);
+#pragma unroll
+                            for (int v = 0; v < 3; ++v) t += ai[3 * q + v] * dist[v];
+                            map[q] = t;
+                        }
+                        R f[3][D];
+#pragma unroll
+                        for (int q = 0; q < 3; ++q)
+#pragma unroll
+                            for (int g = 0; g < D; ++g)
+                                f[q][g] = (ORDER == 1) ? (g == 0 ? R(1) : map[q])
+                                                       : mode1d(g, map[q], h[q], alpha[q]);
+#pragma unroll
+                        for (int e = 0; e < CB; ++e) {
+                            R sa = R(0);
+#pragma unroll
+                            for (int a = 0; a < D; ++a) {
+                                R sb = R(0);
+#pragma unroll
+                                for (int b = 0; b < D; ++b) {
+                                    R sc = R(0);
+#pragma unroll
+                                    for (int cc = 0; cc < D; ++cc) sc += f[2][cc] * cp[a][b][cc][e];
+                                    sb += f[1][b] * sc;
+                                }
+                                sa += f[0][a] * sb;
+                            }
+                            ACC::add(gmu, gi, idx[1][j], idx[2][k], d0 + e, wm * sa, scale_mu);
+                        }
+                        if (d0 == 0) ACC::add(gm, gi, idx[1][j], idx[2][k], 0, wm, scale_m);
                     }
-                    R basis[NM];
-                    if (ORDER == 1) {
-                        basis[0] = R(1);
-                        basis[1] = map[0];
-                        basis[2] = map[1];
-                        basis[3] = map[2];
-                        basis[4] = map[0] * map[1];
-                        basis[5] = map[0] * map[2];
-                        basis[6] = map[1] * map[2];
-                        basis[7] = map[0] * map[1] * map[2];
-                    } else {
-                        R f[3][3];
-#pragma unroll
-                        for (int d = 0; d < 3; ++d)
-#pragma unroll
-                            for (int g = 0; g < 3; ++g) f[d][g] = mode1d(g, map[d], h[d], alpha[d]);
-#pragma unroll
-                        for (int r = 0; r < NM; ++r)
-                            basis[r] = f[0][mode_deg(r, 0)] * f[1][mode_deg(r, 1)] * f[2][mode_deg(r, 2)];
-                    }
-#pragma unroll
-                    for (int d = 0; d < NCU; ++d) {
-                        R s = R(0);
-#pragma unroll
-                        for (int r = 0; r < NM; ++r) s += cp[r][d] * basis[r];
-                        ACC::add(gmu, idx[0][i], idx[1][j], idx[2][k], d, wm * s, scale_mu);
-                    }
-                    ACC::add(gm, idx[0][i], idx[1][j], idx[2][k], 0, wm, scale_m);
-                }
+            }
+        }
     }
 }
 
@@ -163,7 +198,6 @@ __global__ void __launch_bounds__(128)
 polypic_g2p_kernel(MeshP mp, int64_t n, PField x, GField u, PField c, int col, int* err)
 {
     constexpr int K = SplineTraits<ORDER>::K;
-    constexpr int NM = (ORDER == 1) ? 8 : 27;
     constexpr int NCU = STAG ? 1 : NC;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
@@ -202,34 +236,72 @@ polypic_g2p_kernel(MeshP mp, int64_t n, PField x, GField u, PField c, int col, i
                 G[d][2][2] = R(0.5) * rh2;
             }
         }
-        R cp[NM][NCU];
-#pragma unroll
-        for (int r = 0; r < NM; ++r)
-#pragma unroll
-            for (int d = 0; d < NCU; ++d) cp[r][d] = R(0);
-#pragma unroll
-        for (int i = 0; i < K; ++i)
-#pragma unroll
-            for (int j = 0; j < K; ++j)
-#pragma unroll
-                for (int k = 0; k < K; ++k) {
-                    R ue[NCU];
-#pragma unroll
-                    for (int d = 0; d < NCU; ++d)
-                        ue[d] = (R)__ldg(u.ptr<GT>(idx[0][i], idx[1][j], idx[2][k], d));
-#pragma unroll
-                    for (int r = 0; r < NM; ++r) {
-                        const R coeff = G[0][mode_deg(r, 0)][i] * G[1][mode_deg(r, 1)][j] *
-                                        G[2][mode_deg(r, 2)][k];
-#pragma unroll
-                        for (int d = 0; d < NCU; ++d) cp[r][d] += coeff * ue[d];
-                    }
-                }
+        // c_(abc) = sum_i G0[a][i] sum_j G1[b][j] sum_k G2[c][k] u_ijk, one
+        // i-plane at a time, the components in passes of CB (27 FP64 modes:
+        // one component per pass)
+        constexpr int D = ORDER + 1;
+        constexpr int CB = (sizeof(R) == 8 && ORDER == 2) ? 1 : NCU;
         const int ncp = STAG ? (col >= 0 ? NC : 1) : NC;
 #pragma unroll
-        for (int r = 0; r < NM; ++r)
+        for (int d0 = 0; d0 < NCU; d0 += CB) {
+            R cp[D][D][D][CB];
 #pragma unroll
-            for (int d = 0; d < NCU; ++d) c.set<PT>(p, r * ncp + (STAG ? col : d), (PT)cp[r][d]);
+            for (int a = 0; a < D; ++a)
+#pragma unroll
+                for (int b = 0; b < D; ++b)
+#pragma unroll
+                    for (int cc = 0; cc < D; ++cc)
+#pragma unroll
+                        for (int e = 0; e < CB; ++e) cp[a][b][cc][e] = R(0);
+#pragma unroll
+            for (int i = 0; i < K; ++i) {
+                R t2[D][D][CB];  // [b][c] of this i-plane
+#pragma unroll
+                for (int b = 0; b < D; ++b)
+#pragma unroll
+                    for (int cc = 0; cc < D; ++cc)
+#pragma unroll
+                        for (int e = 0; e < CB; ++e) t2[b][cc][e] = R(0);
+#pragma unroll
+                for (int j = 0; j < K; ++j) {
+                    R ue[K][CB];
+#pragma unroll
+                    for (int k = 0; k < K; ++k)
+#pragma unroll
+                        for (int e = 0; e < CB; ++e)
+                            ue[k][e] = (R)__ldg(u.ptr<GT>(idx[0][i], idx[1][j], idx[2][k], d0 + e));
+#pragma unroll
+                    for (int cc = 0; cc < D; ++cc)
+#pragma unroll
+                        for (int e = 0; e < CB; ++e) {
+                            R t1 = R(0);
+#pragma unroll
+                            for (int k = 0; k < K; ++k) t1 += G[2][cc][k] * ue[k][e];
+#pragma unroll
+                            for (int b = 0; b < D; ++b) t2[b][cc][e] += G[1][b][j] * t1;
+                        }
+                }
+#pragma unroll
+                for (int a = 0; a < D; ++a)
+#pragma unroll
+                    for (int b = 0; b < D; ++b)
+#pragma unroll
+                        for (int cc = 0; cc < D; ++cc)
+#pragma unroll
+                            for (int e = 0; e < CB; ++e)
+                                cp[a][b][cc][e] += G[0][a][i] * t2[b][cc][e];
+            }
+#pragma unroll
+            for (int a = 0; a < D; ++a)
+#pragma unroll
+                for (int b = 0; b < D; ++b)
+#pragma unroll
+                    for (int cc = 0; cc < D; ++cc)
+#pragma unroll
+                        for (int e = 0; e < CB; ++e)
+                            c.set<PT>(p, mode_of(a, b, cc) * ncp + (STAG ? col : d0 + e),
+                                      (PT)cp[a][b][cc][e]);
+        }
     }
 }
 

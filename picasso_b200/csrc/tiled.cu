@@ -35,7 +35,7 @@ p2g_tiled_kernel(P2GArgs A, int64_t n)
     p2g_item<ORDER, LPP>(A, t, a, b, smem, stage_base);
 }
 
-template <int ORDER>
+template <int ORDER, bool ADV>
 __global__ void __launch_bounds__(kG2PThreads) g2p_tiled_kernel(G2PArgs A, int64_t n)
 {
     extern __shared__ __align__(16) float smem[];
@@ -45,7 +45,7 @@ __global__ void __launch_bounds__(kG2PThreads) g2p_tiled_kernel(G2PArgs A, int64
     }
     int64_t t, a, b;
     if (!item_range(A.tp, blockIdx.x, t, a, b)) return;  // CTA-uniform
-    g2p_item<ORDER, kG2PThreads>(A, t, a, b, reinterpret_cast<float4*>(smem), threadIdx.x);
+    g2p_item<ORDER, kG2PThreads, ADV>(A, t, a, b, reinterpret_cast<float4*>(smem), threadIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -218,14 +218,14 @@ static picasso_status launch_p2g_tiled(const P2GArgs& A, int64_t n, cudaStream_t
     return check_launch();
 }
 
-template <int ORDER>
+template <int ORDER, bool ADV>
 static picasso_status launch_g2p_tiled(const G2PArgs& A, int64_t n, cudaStream_t st)
 {
     const size_t smem = sizeof(float4) * (size_t)A.tp.nodes;
-    PB_CUDA_TRY(cudaFuncSetAttribute(g2p_tiled_kernel<ORDER>,
+    PB_CUDA_TRY(cudaFuncSetAttribute(g2p_tiled_kernel<ORDER, ADV>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int64_t items = item_bound(A.tp, n);
-    g2p_tiled_kernel<ORDER><<<(unsigned)(items ? items : 1), kG2PThreads, smem, st>>>(A, n);
+    g2p_tiled_kernel<ORDER, ADV><<<(unsigned)(items ? items : 1), kG2PThreads, smem, st>>>(A, n);
     return check_launch();
 }
 
@@ -264,7 +264,8 @@ picasso_status apic_p2g_tiled(const MeshP& mp, int order, int ncomp, Form form, 
 
 picasso_status apic_g2p_tiled(const MeshP& mp, int order, int ncomp, bool f32, int64_t n,
                               const PField& x, const GField& u, const PField& c,
-                              const picasso_bins& bins, int* err, cudaStream_t st, bool* handled)
+                              const picasso_bins& bins, int* err, const Advect* adv,
+                              cudaStream_t st, bool* handled)
 {
     *handled = false;
     if (!f32 || ncomp != 3 || !packed_x(x) || !packed_c(c)) return PICASSO_OK;
@@ -278,9 +279,16 @@ picasso_status apic_g2p_tiled(const MeshP& mp, int order, int ncomp, bool f32, i
     A.u = u;
     A.c = reinterpret_cast<float*>(c.data);
     A.err = err;
-    if (order == 1) return launch_g2p_tiled<1>(A, n, st);
-    if (order == 2) return launch_g2p_tiled<2>(A, n, st);
-    return launch_g2p_tiled<3>(A, n, st);
+    A.x_out = adv ? reinterpret_cast<double*>(x.data) : nullptr;
+    A.adv = adv ? *adv : Advect{};
+    if (adv) {
+        if (order == 1) return launch_g2p_tiled<1, true>(A, n, st);
+        if (order == 2) return launch_g2p_tiled<2, true>(A, n, st);
+        return launch_g2p_tiled<3, true>(A, n, st);
+    }
+    if (order == 1) return launch_g2p_tiled<1, false>(A, n, st);
+    if (order == 2) return launch_g2p_tiled<2, false>(A, n, st);
+    return launch_g2p_tiled<3, false>(A, n, st);
 }
 
 }  // namespace pb

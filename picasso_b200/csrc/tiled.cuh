@@ -26,6 +26,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "gridops.cuh"
 #include "transfer.cuh"
 
 namespace pb {
@@ -70,6 +71,8 @@ struct G2PArgs {
     GField u;
     float* c;
     int* err;
+    double* x_out;  // G2P with advection: positions updated in place (= x)
+    Advect adv;
 };
 
 __device__ __forceinline__ int bin_of(const MeshP& mp, const TileP& tp, int d, int s0)
@@ -511,7 +514,10 @@ __device__ void p2g_item(const P2GArgs& A, int64_t t, int64_t a, int64_t b, floa
 // ---------------------------------------------------------------------------
 // One G2P work item by NTHR threads (a warp or a CTA) sharing `tile`
 // (tp.nodes float4).  Threads are numbered tid in [0, NTHR).
-template <int ORDER, int NTHR>
+// ADV: each particle is then moved, x += dt u_p (FP64, as picasso_advect).
+// The positions of the item's first and last particle are read before the
+// tile barrier, so no thread reads a position another thread has moved.
+template <int ORDER, int NTHR, bool ADV = false>
 __device__ void g2p_item(const G2PArgs& A, int64_t t, int64_t a, int64_t b, float4* tile,
                          int tid)
 {
@@ -632,6 +638,11 @@ __device__ void g2p_item(const G2PArgs& A, int64_t t, int64_t a, int64_t b, floa
         out[0] = make_float4(up[0], up[1], up[2], B[0][0]);
         out[1] = make_float4(B[1][0], B[2][0], B[0][1], B[1][1]);
         out[2] = make_float4(B[2][1], B[0][2], B[1][2], B[2][2]);
+        if constexpr (ADV) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d)
+                A.x_out[3 * p + d] = advect_coord(A.adv, d, xp[d], (double)up[d]);
+        }
     }
 }
 
