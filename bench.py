@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--order", type=int, default=2)
     ap.add_argument("--workload", default="clustered", choices=["clustered", "uniform"])
     ap.add_argument("--tile", type=int, nargs=3, default=[4, 8, 8])
-    ap.add_argument("--chunk", type=int, default=2048, help="particles per work item")
+    ap.add_argument("--chunk", type=int, default=4096, help="particles per work item")
     ap.add_argument("--p2g-lanes", type=int, default=0,
                     help="lanes per particle of the tiled P2G (0 = library choice)")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 plain leg")
@@ -515,7 +515,7 @@ def run_advect(args, peak):
                     ev[i].record()
             mark(0)
             sd0 = pb.create_spline(loc, 3, mesh, state["x"])
-            _, perm, bins = pb.cell_sort(sd0, tuple(args.adv_tile), chunk=2048,
+            _, perm, bins = pb.cell_sort(sd0, tuple(args.adv_tile), chunk=4096,
                                          p2g_lanes=4 if f32 else 0)
             mark(1)
             state["x"], state["m"], state["c"] = pb.permute_members(

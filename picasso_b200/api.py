@@ -402,7 +402,7 @@ class Bins:
         return self.desc.num_tiles[0] * self.desc.num_tiles[1] * self.desc.num_tiles[2]
 
 
-def cell_sort(sd, tile=(4, 8, 8), chunk=2048, stream=None, workspace=None, p2g_lanes=0):
+def cell_sort(sd, tile=(4, 8, 8), chunk=4096, stream=None, workspace=None, p2g_lanes=0):
     """Stable sort of the spline's particles by (tile, bin).  Returns
     (key, perm, bins): keys and permutation as int32 tensors holding uint32
     values, and the Bins to pass to the transfers once the particle members

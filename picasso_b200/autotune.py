@@ -27,7 +27,7 @@ import torch
 from . import api, workloads
 
 TILES = [(4, 4, 4), (4, 4, 8), (4, 8, 8), (8, 8, 8)]
-CHUNKS = [512, 2048]
+CHUNKS = [1024, 4096]
 EDGE_BUCKETS = [(0, 32), (33, 64), (65, 1 << 20)]
 PPC_BUCKETS = [(0, 4), (5, 10), (11, 1 << 20)]
 

@@ -261,9 +261,10 @@ struct BatchShape {
                                                                           : 128;
     // a single-variant precision-form P2G kernel gets the occupancy of the
     // single-call kernel of that variant
-    static constexpr int p2g_lanes = (VAR >= 0 && F32) ? kVarLanes[VAR] : 1;
     static constexpr int min_blocks =
-        threads == 32 ? (p2g_lanes == 1 ? 8 : (p2g_lanes == 2 ? 12 : 16))
+        threads == 32 ? ((VAR >= 0 && F32) ? P2GOccupancy<kVarOrder[VAR >= 0 ? VAR : 0],
+                                                          kVarLanes[VAR >= 0 ? VAR : 0]>::value
+                                           : 8)
                       : (!F32 && threads == 128 ? 3 : 4);
 };
 

@@ -13,15 +13,8 @@ namespace pb {
 
 constexpr int kG2PThreads = 128;
 
-// Registers: 1 lane per particle holds 4 x K^3 accumulators (255 registers,
-// 8 warps per SM); 2 and 4 lanes hold half and a quarter of them.
-template <int LPP>
-struct P2GOccupancy {
-    static constexpr int value = LPP == 1 ? 8 : (LPP == 2 ? 12 : 16);
-};
-
 template <int ORDER, int LPP>
-__global__ void __launch_bounds__(32, P2GOccupancy<LPP>::value)
+__global__ void __launch_bounds__(32, (P2GOccupancy<ORDER, LPP>::value))
 p2g_tiled_kernel(P2GArgs A, int64_t n)
 {
     extern __shared__ __align__(16) float smem[];

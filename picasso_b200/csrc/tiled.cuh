@@ -190,12 +190,27 @@ struct P2GCfg {
     // float4 stores of 8 staged lanes on distinct banks
     static constexpr int SS = ((SV / 4) % 2 == 0) ? SV + 4 : SV;
     static constexpr int R = (SV + 31) / 32;  // merge rounds per staged lane
+    // k-plane merges (a lane's bin advanced by one along k): the K^2 nodes of
+    // the stencil's first k-plane, F fields, packed
+    static constexpr int PV = F * K * K;
+    static constexpr int PV4 = (PV + 3) & ~3;
+    static constexpr int PS = ((PV4 / 4) % 2 == 0) ? PV4 + 4 : PV4;
+    static constexpr int RP = (PV + 31) / 32;
+    static_assert(PS <= SS, "a plane stages inside a full stage slot");
     // ring per stage: x (6 floats) | c (12 floats) | m (1 float) per run
     static constexpr int RING_X = 0, RING_C = 6 * RUNS, RING_M = 18 * RUNS;
     static constexpr int RING = 19 * RUNS + ((19 * RUNS) % 4 ? 4 - (19 * RUNS) % 4 : 0);
     static constexpr int STAGE_OFF = kRing * RING;
     static constexpr int TILE_OFF = STAGE_OFF + kStageLanes * SS;
     static_assert(LPP == 1 || LPP == 2 || LPP == 4, "1, 2 or 4 lanes per particle");
+};
+
+// Single-warp CTAs per SM the P2G register budget is sized for: 1 lane per
+// particle holds 4 x K^3 accumulators (~255 registers), 2 and 4 lanes a half
+// and a quarter of them; cubic 4-lane items also hold a 64-node stencil.
+template <int ORDER, int LPP>
+struct P2GOccupancy {
+    static constexpr int value = LPP == 1 ? 8 : (LPP == 2 ? 12 : (ORDER == 3 ? 12 : 16));
 };
 
 template <int ORDER, int LPP>
@@ -280,6 +295,43 @@ struct P2GAcc {
                 *reinterpret_cast<float4*>(st + f * C::FS + 4 * q) = v;
             }
     }
+
+    // value v of the first k-plane: field v / K^2, node (i, j, 0) with
+    // i * K + j = v % K^2
+    __device__ __forceinline__ float plane_value(int v) const
+    {
+        constexpr int K = C::K;
+        return acc[v / (K * K)][(v % (K * K)) * K];
+    }
+
+    // st[v] <- plane_value(v) with 16-byte stores.
+    __device__ __forceinline__ void stage_plane(float* st) const
+    {
+#pragma unroll
+        for (int q = 0; q < C::PV4 / 4; ++q) {
+            float4 v;
+            v.x = (4 * q + 0 < C::PV) ? plane_value(4 * q + 0) : 0.f;
+            v.y = (4 * q + 1 < C::PV) ? plane_value(4 * q + 1) : 0.f;
+            v.z = (4 * q + 2 < C::PV) ? plane_value(4 * q + 2) : 0.f;
+            v.w = (4 * q + 3 < C::PV) ? plane_value(4 * q + 3) : 0.f;
+            *reinterpret_cast<float4*>(st + 4 * q) = v;
+        }
+    }
+
+    // Moves the sums one node down along k (the stencil moved up by one):
+    // planes 1 .. K-1 become 0 .. K-2, the last plane starts at zero.
+    __device__ __forceinline__ void shift_k()
+    {
+        constexpr int K = C::K;
+#pragma unroll
+        for (int f = 0; f < C::F; ++f)
+#pragma unroll
+            for (int ij = 0; ij < K * K; ++ij) {
+#pragma unroll
+                for (int k = 0; k + 1 < K; ++k) acc[f][ij * K + k] = acc[f][ij * K + k + 1];
+                acc[f][ij * K + K - 1] = 0.f;
+            }
+    }
 };
 
 // Merge plan of one lane: staged value v = lane + 32 r of a staged lane that
@@ -289,8 +341,10 @@ template <int ORDER, int LPP>
 struct MergePlan {
     using C = P2GCfg<ORDER, LPP>;
     int moff[C::R];
-    int fstride;     // F * P
-    unsigned valid;  // bit r: value lane + 32 r exists
+    int poff[C::RP];  // the same for the values of a k-plane stage
+    int fstride;      // F * P
+    unsigned valid;   // bit r: value lane + 32 r exists
+    unsigned pvalid;
     __device__ __forceinline__ void init(const TileP& tp, int lane)
     {
         constexpr int K = C::K;
@@ -305,6 +359,17 @@ struct MergePlan {
                 const int a = nn / (K * K), b = (nn / K) % K, c = nn % K;
                 moff[r] = fs * tp.P + a * tp.SI + b * tp.SJ + c;
                 valid |= 1u << r;
+            }
+        }
+        pvalid = 0;
+#pragma unroll
+        for (int r = 0; r < C::RP; ++r) {
+            const int v = lane + 32 * r;
+            poff[r] = 0;
+            if (v < C::PV) {
+                const int fs = v / (K * K), ij = v % (K * K);
+                poff[r] = fs * tp.P + (ij / K) * tp.SI + (ij % K) * tp.SJ;
+                pvalid |= 1u << r;
             }
         }
     }
@@ -346,6 +411,46 @@ __device__ __forceinline__ void merge_partials(unsigned mask, P2GAcc<ORDER, LPP>
 #pragma unroll
             for (int r = 0; r < C::R; ++r)
                 if ((plan.valid >> r) & 1u) tile[base + plan.moff[r]] += st[lane + 32 * r];
+            __syncwarp();
+        }
+    }
+}
+
+// Lanes in `mask` (whose bin moved one step along k) hand the first k-plane
+// of their sums to the node tile in lane order and shift the rest down.
+template <int ORDER, int LPP>
+__device__ __forceinline__ void merge_plane(unsigned mask, P2GAcc<ORDER, LPP>& acc, int cur_base,
+                                            const MergePlan<ORDER, LPP>& plan, float* tile,
+                                            float* stage, int* stage_base, int lane)
+{
+    using C = P2GCfg<ORDER, LPP>;
+    while (mask) {
+        unsigned batch = mask;
+        if (__popc(mask) > kStageLanes) {
+            batch = 0;
+            unsigned mm = mask;
+#pragma unroll
+            for (int q = 0; q < kStageLanes; ++q) {
+                batch |= mm & (~mm + 1u);
+                mm &= mm - 1u;
+            }
+        }
+        mask &= ~batch;
+        if ((batch >> lane) & 1u) {
+            const int slot = __popc(batch & ((1u << lane) - 1u));
+            acc.stage_plane(stage + slot * C::PS);
+            stage_base[slot] = cur_base | ((lane % LPP) << 28);
+            acc.shift_k();
+        }
+        __syncwarp();
+        const int nstage = __popc(batch);
+        for (int q = 0; q < nstage; ++q) {
+            const float* st = stage + q * C::PS;
+            const int sb = stage_base[q];
+            const int base = (sb & 0x0FFFFFFF) + (LPP > 1 ? (sb >> 28) * plan.fstride : 0);
+#pragma unroll
+            for (int r = 0; r < C::RP; ++r)
+                if ((plan.pvalid >> r) & 1u) tile[base + plan.poff[r]] += st[lane + 32 * r];
             __syncwarp();
         }
     }
@@ -402,59 +507,80 @@ __device__ void p2g_item(const P2GArgs& A, int64_t t, int64_t a, int64_t b, floa
 #pragma unroll
     for (int q = 0; q < kRing - 1; ++q) issue(q);
 
+    // Spline and bin of one particle.  The loop is software-pipelined:
+    // particle s + 1 is located while particle s is accumulated, so that the
+    // serial spline chain of one particle (FP64 logical coordinate, floor,
+    // weights) overlaps the independent multiply-adds of the other.  The
+    // particle's velocity and affine rows are read from the ring when it is
+    // accumulated (its slot is refilled one step later).
+    struct Part {
+        Spline1D<ORDER, float> sp[3];
+        int lb[3];
+        bool ok;
+    };
+    auto locate_slot = [&](int q, Part& P) {
+        P.ok = false;
+        P.lb[0] = P.lb[1] = P.lb[2] = 0;
+        if (q >= cnt) return;
+        const double* sx = reinterpret_cast<const double*>(slot(q) + C::RING_X + run * 6);
+        const double xp[3] = {sx[0], sx[1], sx[2]};
+        P.ok = locate<ORDER>(mp, tp, xp, ob, P.sp, P.lb);
+        if (!P.ok && A.err && h == 0) atomicAdd(A.err, 1);
+    };
+    auto coefficients = [&](int q, float co[C::F][4], float& mass) {
+        const float* sl = slot(q);
+        const float* sc = sl + C::RING_C + run * 12;
+        float cp[12];  // cp[r * 3 + d] = c_p(r, d)
+#pragma unroll
+        for (int v = 0; v < 3; ++v) {
+            const float4 w = *reinterpret_cast<const float4*>(sc + 4 * v);
+            cp[4 * v] = w.x;
+            cp[4 * v + 1] = w.y;
+            cp[4 * v + 2] = w.z;
+            cp[4 * v + 3] = w.w;
+        }
+        mass = sl[C::RING_M + run];
+#pragma unroll
+        for (int f = 0; f < C::F; ++f) {
+            const int g = h * C::F + f;  // global field
+            if (g == 0) {
+                co[f][0] = 1.f;
+                co[f][1] = co[f][2] = co[f][3] = 0.f;
+            } else {
+                const int d = g - 1;
+                co[f][0] = d == 0 ? cp[0] : (d == 1 ? cp[1] : cp[2]);
+                co[f][1] = D * (d == 0 ? cp[3] : (d == 1 ? cp[4] : cp[5]));
+                co[f][2] = D * (d == 0 ? cp[6] : (d == 1 ? cp[7] : cp[8]));
+                co[f][3] = D * (d == 0 ? cp[9] : (d == 1 ? cp[10] : cp[11]));
+            }
+        }
+    };
+
     Acc acc;
     acc.zero();
     int cur = -1, cur_base = 0;
     int bmin[3] = {1 << 30, 1 << 30, 1 << 30}, bmax[3] = {-1, -1, -1};
+    Part P;
+    cp_async_wait<kRing - 2>();  // particle 0 has landed
+    __syncwarp();
+    locate_slot(0, P);
     for (int s = 0; s < U; ++s) {
         __syncwarp();  // no lane still reads the slot refilled next
         issue(s + kRing - 1);
-        cp_async_wait<kRing - 1>();
-        if (LPP > 1) __syncwarp();  // a run's copies are visible to all its lanes
-        const bool valid = s < cnt;
-        Spline1D<ORDER, float> sp[3];
-        int lb[3] = {0, 0, 0};
-        bool ok = false;
-        float co[C::F][4], mass = 0.f;
-        if (valid) {
-            const float* sl = slot(s);
-            const double* sx = reinterpret_cast<const double*>(sl + C::RING_X + run * 6);
-            const double xp[3] = {sx[0], sx[1], sx[2]};
-            ok = locate<ORDER>(mp, tp, xp, ob, sp, lb);
-            if (!ok && A.err && h == 0) atomicAdd(A.err, 1);
-            const float* sc = sl + C::RING_C + run * 12;
-            float cp[12];
-#pragma unroll
-            for (int q = 0; q < 3; ++q) {
-                const float4 v = *reinterpret_cast<const float4*>(sc + 4 * q);
-                cp[4 * q] = v.x;
-                cp[4 * q + 1] = v.y;
-                cp[4 * q + 2] = v.z;
-                cp[4 * q + 3] = v.w;
-            }
-            mass = sl[C::RING_M + run];
-            // cp[r * 3 + d] = c_p(r, d)
-#pragma unroll
-            for (int f = 0; f < C::F; ++f) {
-                const int g = h * C::F + f;  // global field
-                if (g == 0) {
-                    co[f][0] = 1.f;
-                    co[f][1] = co[f][2] = co[f][3] = 0.f;
-                } else {
-                    const int d = g - 1;
-                    const float vd = d == 0 ? cp[0] : (d == 1 ? cp[1] : cp[2]);
-                    const float b0 = d == 0 ? cp[3] : (d == 1 ? cp[4] : cp[5]);
-                    const float b1 = d == 0 ? cp[6] : (d == 1 ? cp[7] : cp[8]);
-                    const float b2 = d == 0 ? cp[9] : (d == 1 ? cp[10] : cp[11]);
-                    co[f][0] = vd;
-                    co[f][1] = D * b0;
-                    co[f][2] = D * b1;
-                    co[f][3] = D * b2;
-                }
-            }
-        }
+        cp_async_wait<kRing - 2>();  // particle s + 1 has landed
+        __syncwarp();
+        Part Q;
+        locate_slot(s + 1, Q);
+        const bool ok = P.ok;
+        const int* lb = P.lb;
         const int lbin = ok ? (lb[0] * tp.T[1] + lb[1]) * tp.T[2] + lb[2] : -1;
-        const unsigned fm = __ballot_sync(kFull, ok && cur >= 0 && lbin != cur);
+        // a bin change to the next bin along k (same i, j) keeps two thirds
+        // of the stencil: only the finished k-plane is merged
+        const bool chg = ok && cur >= 0 && lbin != cur;
+        const bool kstep = chg && lbin == cur + 1 && lb[2] != 0;
+        const unsigned pm = __ballot_sync(kFull, kstep);
+        const unsigned fm = __ballot_sync(kFull, chg && !kstep);
+        if (pm) merge_plane<ORDER, LPP>(pm, acc, cur_base, plan, tile, stage, stage_base, lane);
         if (fm) merge_partials<ORDER, LPP>(fm, acc, cur_base, plan, tile, stage, stage_base, lane);
         if (ok) {
             if (lbin != cur) {
@@ -466,8 +592,11 @@ __device__ void p2g_item(const P2GArgs& A, int64_t t, int64_t a, int64_t b, floa
                     bmax[d] = max(bmax[d], lb[d]);
                 }
             }
-            acc.add(sp, mass, co);
+            float co[C::F][4], mass;
+            coefficients(s, co, mass);
+            acc.add(P.sp, mass, co);
         }
+        P = Q;
     }
     cp_async_wait<0>();
     const unsigned fm = __ballot_sync(kFull, cur >= 0);
