@@ -60,6 +60,40 @@ __global__ void advect_kernel(int64_t n, PField x, PField c, Advect a)
 
 using namespace pb;
 
+// Fill of a contiguous element range: 16-byte stores (the array start is
+// element-aligned; a scalar head and tail handle the unaligned ends).
+template <class T>
+__global__ void fill_contiguous_kernel(T* data, int64_t n, T v)
+{
+    constexpr int V = 16 / sizeof(T);
+    const uintptr_t addr = reinterpret_cast<uintptr_t>(data);
+    const int64_t h0 = (int64_t)(((16 - addr % 16) % 16) / sizeof(T));
+    const int64_t head = n < h0 ? n : h0;
+    const int64_t nvec = (n - head) / V;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t t0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t0 < head) data[t0] = v;
+    struct alignas(16) Vec {
+        T e[V];
+    };
+    Vec w;
+#pragma unroll
+    for (int q = 0; q < V; ++q) w.e[q] = v;
+    Vec* vd = reinterpret_cast<Vec*>(data + head);
+    for (int64_t i = t0; i < nvec; i += stride) vd[i] = w;
+    const int64_t tail = head + nvec * V;
+    if (t0 < n - tail) data[tail + t0] = v;
+}
+
+// True when the box of ncomp components is one contiguous element range of f
+// (Cabana LayoutRight over the whole local grid).
+static bool contiguous(const Box& b, const GField& f, int ncomp)
+{
+    return (ncomp == 1 || f.s[3] == 1) && f.s[2] == ncomp && f.s[1] == (int64_t)b.n[2] * ncomp &&
+           f.s[0] == (int64_t)b.n[1] * b.n[2] * ncomp && b.lo[0] == 0 && b.lo[1] == 0 &&
+           b.lo[2] == 0;
+}
+
 extern "C" picasso_status picasso_grid_fill(const picasso_mesh* mesh, int32_t ncomp,
                                             picasso_grid_field f, double value,
                                             const picasso_exec* exec)
@@ -73,6 +107,26 @@ extern "C" picasso_status picasso_grid_fill(const picasso_mesh* mesh, int32_t nc
     Box b = full_box(*mesh);
     GField g = make_gfield(f);
     cudaStream_t s = stream_of(exec);
+    if (contiguous(b, g, ncomp)) {
+        const int64_t n = b.count() * ncomp;
+        const unsigned blocks = grid_for(n / 2, 256, 148LL * 16);
+        if (f.dtype == PICASSO_F64) {
+            if (value == 0.0) PB_CUDA_TRY(cudaMemsetAsync(f.data, 0, n * sizeof(double), s));
+            else fill_contiguous_kernel<double><<<blocks, 256, 0, s>>>((double*)f.data, n, value);
+        } else if (f.dtype == PICASSO_F32) {
+            if (value == 0.0) PB_CUDA_TRY(cudaMemsetAsync(f.data, 0, n * sizeof(float), s));
+            else
+                fill_contiguous_kernel<float><<<blocks, 256, 0, s>>>((float*)f.data, n,
+                                                                     (float)value);
+        } else {
+            const long long q = llrint(ldexp(value, f.fixed_bits));
+            if (q == 0) PB_CUDA_TRY(cudaMemsetAsync(f.data, 0, n * sizeof(long long), s));
+            else
+                fill_contiguous_kernel<long long><<<blocks, 256, 0, s>>>((long long*)f.data,
+                                                                         n, q);
+        }
+        return check_launch();
+    }
     const unsigned blocks = grid_for(b.count() * ncomp, 256, 148LL * 32);
     if (f.dtype == PICASSO_F64)
         fill_kernel<double><<<blocks, 256, 0, s>>>(b, g, ncomp, value);

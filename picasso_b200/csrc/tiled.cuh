@@ -32,7 +32,6 @@
 namespace pb {
 
 constexpr int kStageLanes = 8;  // lanes staged per merge round
-constexpr int kRing = 3;        // particle records in flight per run
 constexpr unsigned kFull = 0xFFFFFFFFu;
 
 struct TileP {
@@ -200,7 +199,12 @@ struct P2GCfg {
     // ring per stage: x (6 floats) | c (12 floats) | m (1 float) per run
     static constexpr int RING_X = 0, RING_C = 6 * RUNS, RING_M = 18 * RUNS;
     static constexpr int RING = 19 * RUNS + ((19 * RUNS) % 4 ? 4 - (19 * RUNS) % 4 : 0);
-    static constexpr int STAGE_OFF = kRing * RING;
+    // ring depth: records of DEPTH - 1 particles are in flight per run; the
+    // warps with fewer runs (more lanes per particle) need more to keep the
+    // same bytes in flight.  Deeper rings cost shared memory, which costs
+    // warps (measured: depth 4 fastest for one lane per particle).
+    static constexpr int DEPTH = LPP == 1 ? 4 : (LPP == 2 ? 8 : 10);
+    static constexpr int STAGE_OFF = DEPTH * RING;
     static constexpr int TILE_OFF = STAGE_OFF + kStageLanes * SS;
     static_assert(LPP == 1 || LPP == 2 || LPP == 4, "1, 2 or 4 lanes per particle");
 };
@@ -485,7 +489,7 @@ __device__ void p2g_item(const P2GArgs& A, int64_t t, int64_t a, int64_t b, floa
     plan.init(tp, lane);
     const float D = (ORDER >= 2) ? inertial_scaling<ORDER, float>(mp.dx[0]) : 1.f;
 
-    auto slot = [&](int q) { return ring + (q % kRing) * C::RING; };
+    auto slot = [&](int q) { return ring + (q % C::DEPTH) * C::RING; };
     // the 7 copies of a particle record (x0..x2, c0..c2, m) are spread over
     // the run's lanes: copy j is issued by lane h == j % LPP
     auto issue = [&](int q) {
@@ -505,14 +509,10 @@ __device__ void p2g_item(const P2GArgs& A, int64_t t, int64_t a, int64_t b, floa
         cp_async_commit();
     };
 #pragma unroll
-    for (int q = 0; q < kRing - 1; ++q) issue(q);
+    for (int q = 0; q < C::DEPTH - 1; ++q) issue(q);
 
-    // Spline and bin of one particle.  The loop is software-pipelined:
-    // particle s + 1 is located while particle s is accumulated, so that the
-    // serial spline chain of one particle (FP64 logical coordinate, floor,
-    // weights) overlaps the independent multiply-adds of the other.  The
-    // particle's velocity and affine rows are read from the ring when it is
-    // accumulated (its slot is refilled one step later).
+    // Spline and bin of one particle, and its mass and coefficients, read
+    // from its ring slot.
     struct Part {
         Spline1D<ORDER, float> sp[3];
         int lb[3];
@@ -560,17 +560,13 @@ __device__ void p2g_item(const P2GArgs& A, int64_t t, int64_t a, int64_t b, floa
     acc.zero();
     int cur = -1, cur_base = 0;
     int bmin[3] = {1 << 30, 1 << 30, 1 << 30}, bmax[3] = {-1, -1, -1};
-    Part P;
-    cp_async_wait<kRing - 2>();  // particle 0 has landed
-    __syncwarp();
-    locate_slot(0, P);
     for (int s = 0; s < U; ++s) {
         __syncwarp();  // no lane still reads the slot refilled next
-        issue(s + kRing - 1);
-        cp_async_wait<kRing - 2>();  // particle s + 1 has landed
-        __syncwarp();
-        Part Q;
-        locate_slot(s + 1, Q);
+        issue(s + C::DEPTH - 1);
+        cp_async_wait<C::DEPTH - 1>();  // record s has landed
+        __syncwarp();                   // ... for every lane of its run
+        Part P;
+        locate_slot(s, P);
         const bool ok = P.ok;
         const int* lb = P.lb;
         const int lbin = ok ? (lb[0] * tp.T[1] + lb[1]) * tp.T[2] + lb[2] : -1;
@@ -596,7 +592,6 @@ __device__ void p2g_item(const P2GArgs& A, int64_t t, int64_t a, int64_t b, floa
             coefficients(s, co, mass);
             acc.add(P.sp, mass, co);
         }
-        P = Q;
     }
     cp_async_wait<0>();
     const unsigned fm = __ballot_sync(kFull, cur >= 0);

@@ -117,3 +117,35 @@ def test_mat3_inverse(cuda):
     assert rel_err(inv.cpu().numpy(), inv_o) <= 1e-12
     cond_ok = np.abs(det_o) > 1e-3
     np.testing.assert_allclose(y.cpu().numpy()[cond_ok], x0[cond_ok], rtol=0, atol=1e-11)
+
+
+@pytest.mark.parametrize("kind", ["f64", "f32", "fixed"])
+@pytest.mark.parametrize("value", [0.0, 1.25])
+def test_grid_fill_contiguous_and_strided(cuda, kind, value):
+    """Fill of a whole (nx, ny, nz, c) array (one contiguous range: memset or
+    vector stores, odd element counts and an offset start included) and of a
+    strided component view (element by element)."""
+    from picasso_b200 import FixedGrid, grid_fill
+    mesh = periodic_mesh(7, halo=1)
+    desc = mesh.descriptor(FieldLocation.Node)
+    ext = mesh.extent(FieldLocation.Node)
+    dt = {"f64": torch.float64, "f32": torch.float32, "fixed": torch.int64}[kind]
+    raw = torch.full((1,) + ext + (3,), 7, dtype=dt, device="cuda")
+    whole = raw[0] if kind != "fixed" else FixedGrid(raw[0], 20)
+    grid_fill(desc, whole, value, ncomp=3)
+    part = torch.full(ext + (3,), 7, dtype=dt, device="cuda")
+    comp = part[..., 1] if kind != "fixed" else FixedGrid(part[..., 1], 20)
+    grid_fill(desc, comp, value, ncomp=1)
+    torch.cuda.synchronize()
+    expect = value if kind != "fixed" else int(round(value * 2 ** 20))
+    assert bool((raw == expect).all())
+    assert bool((part[..., 1] == expect).all())
+    assert bool((part[..., 0] == 7).all()) and bool((part[..., 2] == 7).all())
+    # an odd-sized contiguous range that starts off a 16-byte boundary
+    buf = torch.full((1 + 5 * 5 * 5 * 1,), 7, dtype=dt, device="cuda")
+    small = UniformMesh([0, 0, 0, 1, 1, 1], cell_size=0.2, periodic=(True,) * 3)
+    view = buf[1:].view(5, 5, 5)
+    grid_fill(small.descriptor(FieldLocation.Node),
+              view if kind != "fixed" else FixedGrid(view, 20), value, ncomp=1)
+    torch.cuda.synchronize()
+    assert int(buf[0]) == 7 and bool((buf[1:] == expect).all())
