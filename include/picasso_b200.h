@@ -249,6 +249,36 @@ PICASSO_API picasso_status picasso_grid_velocity(const picasso_mesh* mesh, int32
                                      double mass_threshold, picasso_grid_field u_i,
                                      picasso_grid_field u64_i, const picasso_exec* exec);
 
+/* Grid update ("field solve" of the reference's explicit APIC time step,
+ * doc/basic/explict_nearly_incompressible_flow.md:20-21):
+ *   u_i = (mu_i + dt f_i) / m_i + dt g   where m_i > mass_threshold, else 0,
+ * then the wall conditions below, on the owned entities (all entities along
+ * non-periodic dimensions).  3 components.  FP64 arithmetic rounded step by
+ * step (no FMA), so results are reproducible bit for bit.  f_i (F64 or the
+ * type of mu_i) is optional (data == NULL: no force).  Walls apply along
+ * non-periodic dimensions to the nodes within wall_width of the owned range's
+ * first / last node (and to the ghost nodes beyond): NO_SLIP sets u = 0,
+ * FREE_SLIP sets the wall-normal component to 0. */
+typedef enum picasso_wall {
+    PICASSO_WALL_NONE = 0,
+    PICASSO_WALL_NO_SLIP = 1,
+    PICASSO_WALL_FREE_SLIP = 2
+} picasso_wall;
+
+typedef struct picasso_grid_update_params {
+    double dt;
+    double gravity[3];
+    double mass_threshold;
+    int32_t wall[3][2];  /* picasso_wall per dimension, low and high side */
+    int32_t wall_width;  /* nodes from the wall the condition covers (>= 0) */
+} picasso_grid_update_params;
+
+PICASSO_API picasso_status picasso_grid_update(const picasso_mesh* mesh, picasso_grid_field m_i,
+                                               picasso_grid_field mu_i, picasso_grid_field f_i,
+                                               const picasso_grid_update_params* params,
+                                               picasso_grid_field u_i, picasso_grid_field u64_i,
+                                               const picasso_exec* exec);
+
 /* Particle advection x_p += dt * c_p(0, :) in FP64, then periodic wrap of the
  * position into the owned box along periodic dimensions. */
 PICASSO_API picasso_status picasso_advect(const picasso_mesh* mesh, int64_t num_particles,

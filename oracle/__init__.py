@@ -47,6 +47,9 @@ def lib():
                                    _abi.GridField, _abi.ParticleField, P(C.c_int64)],
             "oracle_grid_velocity": [P(_abi.Mesh), C.c_int, _abi.GridField, _abi.GridField,
                                      C.c_double, _abi.GridField],
+            "oracle_grid_update": [P(_abi.Mesh), _abi.GridField, _abi.GridField, _abi.GridField,
+                                   C.c_double, P(C.c_double), C.c_double, P(C.c_int), C.c_int,
+                                   _abi.GridField],
             "oracle_advect": [P(_abi.Mesh), C.c_int64, C.c_double, _abi.ParticleField,
                               _abi.ParticleField],
             "oracle_cell_sort": [P(_abi.Spline), C.c_int64, _abi.ParticleField, P(C.c_int),
@@ -130,6 +133,15 @@ def grid_velocity(mesh, m_i, mu_i, u_i, thr=1e-12):
     nc = mu_i.shape[3] if mu_i.ndim == 4 else 1
     _check(lib().oracle_grid_velocity(C.byref(mesh), nc, _gf(m_i), _gf(mu_i), float(thr),
                                       _gf(u_i)), "grid_velocity")
+
+
+def grid_update(mesh, m_i, mu_i, u_i, dt, gravity, f_i=None, thr=1e-12, walls=None, width=1):
+    """walls: ((lo, hi),) * 3 with 0 none, 1 no-slip, 2 free-slip."""
+    w = (C.c_int * 6)(*[(walls[d][s] if walls else 0) for d in range(3) for s in range(2)])
+    g = (C.c_double * 3)(*[float(v) for v in gravity])
+    fi = _gf(f_i) if f_i is not None else _abi.GridField()
+    _check(lib().oracle_grid_update(C.byref(mesh), _gf(m_i), _gf(mu_i), fi, float(dt), g,
+                                    float(thr), w, int(width), _gf(u_i)), "grid_update")
 
 
 def advect(mesh, x, v, dt):

@@ -620,6 +620,43 @@ int oracle_grid_velocity(const picasso_mesh* mesh, int ncomp, picasso_grid_field
     return PICASSO_OK;
 }
 
+/* Grid update of the explicit APIC step, doc/basic/
+ * explict_nearly_incompressible_flow.md:20-21: u = (mu + dt f) / m + dt g where
+ * m > thr, else 0; then u <- BC(u) with walls along non-periodic dimensions
+ * (wall[d][side]: 0 none, 1 no-slip u = 0, 2 free-slip u_d = 0) on the nodes
+ * within `width` of the owned range's ends and beyond.  f may be NULL data. */
+int oracle_grid_update(const picasso_mesh* mesh, picasso_grid_field m_i,
+                       picasso_grid_field mu_i, picasso_grid_field f_i, double dt,
+                       const double g[3], double thr, const int wall[6], int width,
+                       picasso_grid_field u_i)
+{
+    int lo[3], hi[3];
+    owned_box(mesh, lo, hi);
+    for (int i = lo[0]; i < hi[0]; ++i)
+        for (int j = lo[1]; j < hi[1]; ++j)
+            for (int k = lo[2]; k < hi[2]; ++k) {
+                double m = *gref(&m_i, i, j, k, 0);
+                double u[3];
+                for (int d = 0; d < 3; ++d) {
+                    double p = *gref(&mu_i, i, j, k, d);
+                    if (f_i.data) p = p + dt * *gref(&f_i, i, j, k, d);
+                    u[d] = (m > thr) ? p / m + dt * g[d] : 0.0;
+                }
+                const int idx[3] = {i, j, k};
+                for (int d = 0; d < 3; ++d) {
+                    if (mesh->periodic[d]) continue;
+                    int side = -1;
+                    if (idx[d] < mesh->own_begin[d] + width) side = 0;
+                    else if (idx[d] >= mesh->own_begin[d] + mesh->own_extent[d] - width) side = 1;
+                    if (side < 0) continue;
+                    if (wall[2 * d + side] == 1) u[0] = u[1] = u[2] = 0.0;
+                    else if (wall[2 * d + side] == 2) u[d] = 0.0;
+                }
+                for (int d = 0; d < 3; ++d) *gref(&u_i, i, j, k, d) = u[d];
+            }
+    return PICASSO_OK;
+}
+
 int oracle_advect(const picasso_mesh* mesh, int64_t np, double dt,
                   picasso_particle_field x, picasso_particle_field c)
 {

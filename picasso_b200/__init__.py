@@ -26,6 +26,7 @@ from .api import (  # noqa: F401
     fixed_bits_for,
     grid_field,
     grid_fill,
+    grid_update,
     grid_velocity,
     mat3_inverse,
     particle_field,

@@ -66,6 +66,14 @@ class Exec(C.Structure):
                 ("bins", C.POINTER(Bins))]
 
 
+class GridUpdateParams(C.Structure):
+    _fields_ = [("dt", C.c_double), ("gravity", C.c_double * 3), ("mass_threshold", C.c_double),
+                ("wall", (C.c_int32 * 2) * 3), ("wall_width", C.c_int32)]
+
+
+WALL_NONE, WALL_NO_SLIP, WALL_FREE_SLIP = 0, 1, 2
+
+
 class BatchInstance(C.Structure):
     _fields_ = [("spline", Spline), ("num_particles", C.c_int64), ("x_p", ParticleField),
                 ("m_p", ParticleField), ("c_p", ParticleField), ("m_i", GridField),
@@ -103,6 +111,9 @@ SIGNATURES = [
     ("picasso_grid_velocity", C.c_int,
      [C.POINTER(Mesh), C.c_int32, GridField, GridField, C.c_double, GridField, GridField,
       C.POINTER(Exec)]),
+    ("picasso_grid_update", C.c_int,
+     [C.POINTER(Mesh), GridField, GridField, GridField, C.POINTER(GridUpdateParams), GridField,
+      GridField, C.POINTER(Exec)]),
     ("picasso_advect", C.c_int,
      [C.POINTER(Mesh), C.c_int64, C.c_double, ParticleField, ParticleField, C.POINTER(Exec)]),
     ("picasso_apic_g2p_advect", C.c_int,

@@ -376,6 +376,30 @@ def grid_velocity(mesh_desc, m_i, mu_i, u_i, mass_threshold=1e-12, u64_i=None, s
                                        g64, C.byref(ex.desc)), "grid_velocity")
 
 
+def grid_update(mesh_desc, m_i, mu_i, u_i, dt, gravity=(0.0, 0.0, 0.0), f_i=None,
+                mass_threshold=1e-12, walls=None, wall_width=1, u64_i=None, stream=None):
+    """u_i = (mu_i + dt f_i) / m_i + dt g where m_i > threshold (else 0), then
+    wall conditions along non-periodic dimensions: ``walls[d] = (low, high)``
+    with "none", "no_slip" or "free_slip"."""
+    kinds = {"none": _abi.WALL_NONE, "no_slip": _abi.WALL_NO_SLIP,
+             "free_slip": _abi.WALL_FREE_SLIP}
+    prm = _abi.GridUpdateParams()
+    prm.dt = float(dt)
+    for d in range(3):
+        prm.gravity[d] = float(gravity[d])
+        for side in range(2):
+            prm.wall[d][side] = kinds[walls[d][side]] if walls else _abi.WALL_NONE
+    prm.mass_threshold = float(mass_threshold)
+    prm.wall_width = int(wall_width)
+    ex = _exec(stream, None, None)
+    none = _abi.GridField()
+    check(_lib().picasso_grid_update(C.byref(mesh_desc), grid_field(m_i), grid_field(mu_i),
+                                     grid_field(f_i) if f_i is not None else none,
+                                     C.byref(prm), grid_field(u_i),
+                                     grid_field(u64_i) if u64_i is not None else none,
+                                     C.byref(ex.desc)), "grid_update")
+
+
 def advect(mesh_desc, x_p, c_p, dt, stream=None):
     """x_p += dt * c_p(0, :) in FP64 with periodic wrap."""
     ex = _exec(stream, None, None)

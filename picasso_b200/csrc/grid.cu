@@ -45,6 +45,19 @@ static void launch_velocity(int ncomp, Box b, GField gm, GField gmu, GField gu, 
         velocity_kernel<MT, UT, 3><<<blocks, 256, 0, st>>>(b, gm, gmu, gu, gu64, thr, inv_m, inv_mu);
 }
 
+template <class MT, class FT, class UT>
+__global__ void update_kernel(Box b, GridUpdate P, GField gm, GField gmu, GField gf, GField gu,
+                              GField gu64)
+{
+    const int64_t total = b.count();
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        int i, j, k;
+        b.at(e, i, j, k);
+        update_node<MT, FT, UT>(P, gm, gmu, gf, gu, gu64, i, j, k);
+    }
+}
+
 template <class CT>
 __global__ void advect_kernel(int64_t n, PField x, PField c, Advect a)
 {
@@ -173,6 +186,61 @@ extern "C" picasso_status picasso_grid_velocity(const picasso_mesh* mesh, int32_
             launch_velocity<double, double>(ncomp, b, gm, gmu, gu, gu64, mass_threshold, inv_m,
                                             inv_mu, s);
     }
+    return check_launch();
+}
+
+extern "C" picasso_status picasso_grid_update(const picasso_mesh* mesh, picasso_grid_field m_i,
+                                              picasso_grid_field mu_i, picasso_grid_field f_i,
+                                              const picasso_grid_update_params* prm,
+                                              picasso_grid_field u_i, picasso_grid_field u64_i,
+                                              const picasso_exec* exec)
+{
+    picasso_status st = validate_mesh(mesh);
+    if (st) return st;
+    if (!prm || prm->wall_width < 0) return PICASSO_ERR_INVALID_ARGUMENT;
+    for (int d = 0; d < 3; ++d)
+        for (int s = 0; s < 2; ++s)
+            if (prm->wall[d][s] < PICASSO_WALL_NONE || prm->wall[d][s] > PICASSO_WALL_FREE_SLIP)
+                return PICASSO_ERR_INVALID_ARGUMENT;
+    if ((st = validate_gfield(m_i, PICASSO_F64, PICASSO_I64_FIXED))) return st;
+    if ((st = validate_gfield(mu_i, m_i.dtype))) return st;
+    const bool force = f_i.data != nullptr;
+    if (force && (st = validate_gfield(f_i, PICASSO_F64, mu_i.dtype))) return st;
+    if ((st = validate_gfield(u_i, PICASSO_F64, PICASSO_F32))) return st;
+    if (u64_i.data && (st = validate_gfield(u64_i, PICASSO_F64))) return st;
+    GridUpdate P;
+    P.dt = prm->dt;
+    P.thr = prm->mass_threshold;
+    const bool fixed = m_i.dtype == PICASSO_I64_FIXED;
+    P.inv_m = fixed ? ldexp(1.0, -m_i.fixed_bits) : 1.0;
+    P.inv_mu = fixed ? ldexp(1.0, -mu_i.fixed_bits) : 1.0;
+    P.inv_f = (force && f_i.dtype == PICASSO_I64_FIXED) ? ldexp(1.0, -f_i.fixed_bits) : 1.0;
+    P.force = force;
+    for (int d = 0; d < 3; ++d) {
+        P.g[d] = prm->gravity[d];
+        const bool walls = !mesh->periodic[d];
+        P.wall[d][0] = walls ? prm->wall[d][0] : PICASSO_WALL_NONE;
+        P.wall[d][1] = walls ? prm->wall[d][1] : PICASSO_WALL_NONE;
+        P.lo_wall[d] = mesh->own_begin[d] + prm->wall_width;
+        P.hi_wall[d] = mesh->own_begin[d] + mesh->own_extent[d] - prm->wall_width;
+    }
+    Box b = owned_box(*mesh);
+    GField gm = make_gfield(m_i), gmu = make_gfield(mu_i), gf = make_gfield(f_i);
+    GField gu = make_gfield(u_i), gu64 = make_gfield(u64_i);
+    cudaStream_t s = stream_of(exec);
+    const unsigned blocks = grid_for(b.count(), 256, 148LL * 32);
+    const bool f64f = !force || f_i.dtype == PICASSO_F64;
+    const bool u32 = u_i.dtype == PICASSO_F32;
+#define PB_UPD(MT, FT, UT) \
+    update_kernel<MT, FT, UT><<<blocks, 256, 0, s>>>(b, P, gm, gmu, gf, gu, gu64)
+    if (fixed) {
+        if (f64f) { if (u32) PB_UPD(long long, double, float); else PB_UPD(long long, double, double); }
+        else { if (u32) PB_UPD(long long, long long, float); else PB_UPD(long long, long long, double); }
+    } else {
+        if (u32) PB_UPD(double, double, float);
+        else PB_UPD(double, double, double);
+    }
+#undef PB_UPD
     return check_launch();
 }
 

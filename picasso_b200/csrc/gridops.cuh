@@ -60,6 +60,46 @@ __device__ __forceinline__ void velocity_node(const GField& gm, const GField& gm
     }
 }
 
+// Grid update of one node: u = (mu + dt f) / m + dt g where m > thr (else 0),
+// then the wall conditions; FP64 rounded step by step.
+struct GridUpdate {
+    double dt, g[3], thr, inv_m, inv_mu, inv_f;
+    int wall[3][2];
+    int lo_wall[3];  // nodes with index < lo_wall[d] are on the low wall
+    int hi_wall[3];  // nodes with index >= hi_wall[d] are on the high wall
+    bool force;
+};
+
+template <class MT, class FT, class UT>
+__device__ __forceinline__ void update_node(const GridUpdate& P, const GField& gm,
+                                            const GField& gmu, const GField& gf, const GField& gu,
+                                            const GField& gu64, int i, int j, int k)
+{
+    const double m = __dmul_rn((double)*gm.ptr<MT>(i, j, k, 0), P.inv_m);
+    const bool keep = m > P.thr;
+    double u[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        double p = __dmul_rn((double)*gmu.ptr<MT>(i, j, k, c), P.inv_mu);
+        if (P.force) p = __dadd_rn(p, __dmul_rn(P.dt, __dmul_rn((double)*gf.ptr<FT>(i, j, k, c), P.inv_f)));
+        u[c] = keep ? __dadd_rn(__ddiv_rn(p, m), __dmul_rn(P.dt, P.g[c])) : 0.0;
+    }
+    const int idx[3] = {i, j, k};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const int side = idx[d] < P.lo_wall[d] ? 0 : (idx[d] >= P.hi_wall[d] ? 1 : -1);
+        if (side < 0) continue;
+        const int w = P.wall[d][side];
+        if (w == PICASSO_WALL_NO_SLIP) u[0] = u[1] = u[2] = 0.0;
+        else if (w == PICASSO_WALL_FREE_SLIP) u[d] = 0.0;
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        *gu.ptr<UT>(i, j, k, c) = (UT)u[c];
+        if (gu64.data) *gu64.ptr<double>(i, j, k, c) = u[c];
+    }
+}
+
 // Position update x += dt v with periodic wrap into the owned box, FP64,
 // rounded step by step as x + (dt * v) (no FMA, so every path that advects
 // gives the same bits).

@@ -280,6 +280,22 @@ __global__ void permute_kernel(int64_t n, int ncomp, const uint32_t* __restrict_
     }
 }
 
+// Packed rows (array of structures): one thread per (particle, word) with the
+// widest word that divides the row and both base addresses, so that the
+// stores of a warp are contiguous and a row is read in whole words.
+template <class W>
+__global__ void permute_rows_kernel(int64_t n, int words, const uint32_t* __restrict__ perm,
+                                    const W* __restrict__ src, W* __restrict__ dst)
+{
+    const int64_t total = n * words;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t p = e / words;
+        const int w = (int)(e - p * words);
+        dst[e] = src[(int64_t)__ldg(perm + p) * words + w];
+    }
+}
+
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
@@ -448,6 +464,29 @@ extern "C" picasso_status picasso_permute(int64_t num_particles, int32_t ncomp,
     if (src.data == dst.data) return PICASSO_ERR_INVALID_ARGUMENT;
     if (num_particles == 0) return PICASSO_OK;
     cudaStream_t s = stream_of(exec);
+    const int64_t esize = src.dtype == PICASSO_F64 ? 8 : 4;
+    auto packed = [&](const picasso_particle_field& f) {
+        return (f.vector_shift == 0 && f.tile_stride == ncomp && (f.comp_stride == 1 || ncomp == 1)) ||
+               (ncomp == 1 && f.vector_shift >= 62);
+    };
+    if (packed(src) && packed(dst)) {
+        const int64_t row = esize * ncomp;
+        const uintptr_t al = reinterpret_cast<uintptr_t>(src.data) | reinterpret_cast<uintptr_t>(dst.data);
+        const int64_t word = (row % 16 == 0 && al % 16 == 0) ? 16 : ((row % 8 == 0 && al % 8 == 0) ? 8 : 4);
+        const int words = (int)(row / word);
+        const unsigned blocks = grid_for(num_particles * words, 256);
+        if (word == 16)
+            permute_rows_kernel<uint4><<<blocks, 256, 0, s>>>(num_particles, words, perm,
+                                                              (const uint4*)src.data, (uint4*)dst.data);
+        else if (word == 8)
+            permute_rows_kernel<uint2><<<blocks, 256, 0, s>>>(num_particles, words, perm,
+                                                              (const uint2*)src.data, (uint2*)dst.data);
+        else
+            permute_rows_kernel<uint32_t><<<blocks, 256, 0, s>>>(num_particles, words, perm,
+                                                                 (const uint32_t*)src.data,
+                                                                 (uint32_t*)dst.data);
+        return check_launch();
+    }
     const unsigned blocks = grid_for(num_particles, 256);
     if (src.dtype == PICASSO_F64)
         permute_kernel<double><<<blocks, 256, 0, s>>>(num_particles, ncomp, perm, make_pfield(src),

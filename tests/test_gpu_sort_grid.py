@@ -69,6 +69,16 @@ def test_permute(cuda):
     assert torch.equal(dst, src[perm.long()])
     s32 = src.float()
     assert torch.equal(permute(perm, s32), s32[perm.long()])
+    # packed rows of 24 B (8-byte words), 4 B and 8 B scalars, and a strided
+    # view (element-wise path)
+    x = _dev(rng.standard_normal((1000, 3)))
+    assert torch.equal(permute(perm, x), x[perm.long()])
+    m32 = s32[:, 0, 0].contiguous()
+    assert torch.equal(permute(perm, m32), m32[perm.long()])
+    m64 = src[:, 0, 0].contiguous()
+    assert torch.equal(permute(perm, m64), m64[perm.long()])
+    strided = src[:, 1:3, :]
+    assert torch.equal(permute(perm, strided), strided[perm.long()])
 
 
 def test_grid_velocity_vs_oracle(cuda):
@@ -149,3 +159,49 @@ def test_grid_fill_contiguous_and_strided(cuda, kind, value):
               view if kind != "fixed" else FixedGrid(view, 20), value, ncomp=1)
     torch.cuda.synchronize()
     assert int(buf[0]) == 7 and bool((buf[1:] == expect).all())
+
+
+@pytest.mark.parametrize("storage", ["f64", "fixed"])
+@pytest.mark.parametrize("walls", [None, (("no_slip", "free_slip"), ("free_slip", "none"),
+                                          ("none", "no_slip"))])
+def test_grid_update_vs_oracle(cuda, storage, walls):
+    """Field solve u = (mu + dt f) / m + dt g (m > 1e-12) with wall conditions
+    on a non-periodic Node mesh, against the oracle: bit-identical FP64."""
+    from picasso_b200 import FixedGrid, grid_update
+    mesh = UniformMesh([0, 0, 0, 1, 1, 1], cell_size=1 / 10, periodic=(False, True, False),
+                       halo_cell_width=2)
+    loc = FieldLocation.Node
+    ext = mesh.extent(loc)
+    rng = np.random.default_rng(700)
+    m = rng.uniform(0.0, 2.0, ext)
+    m[rng.random(ext) < 0.2] = 0.0  # empty nodes
+    mu = rng.standard_normal(ext + (3,))
+    f = rng.standard_normal(ext + (3,))
+    bits = 30
+    if storage == "fixed":  # values representable in the fixed-point format
+        m = np.round(m * 2 ** bits) / 2 ** bits
+        mu = np.round(mu * 2 ** bits) / 2 ** bits
+    dt, g = 0.01, (0.0, -9.81, 0.5)
+    code = {"none": 0, "no_slip": 1, "free_slip": 2}
+    wcodes = [[code[w] for w in pair] for pair in walls] if walls else None
+    desc = mesh.descriptor(loc)
+    u_o = np.zeros(ext + (3,))
+    oracle.grid_update(desc, m, mu, u_o, dt, g, f_i=f, thr=1e-12, walls=wcodes, width=2)
+    if storage == "fixed":
+        gm = FixedGrid(torch.as_tensor(np.round(m * 2 ** bits).astype(np.int64), device="cuda"),
+                       bits)
+        gmu = FixedGrid(torch.as_tensor(np.round(mu * 2 ** bits).astype(np.int64),
+                                        device="cuda"), bits)
+    else:
+        gm, gmu = torch.as_tensor(m, device="cuda"), torch.as_tensor(mu, device="cuda")
+    u = torch.full(ext + (3,), 5.0, dtype=torch.float64, device="cuda")
+    u32 = torch.zeros(ext + (3,), dtype=torch.float32, device="cuda")
+    grid_update(desc, gm, gmu, u32, dt, g, f_i=torch.as_tensor(f, device="cuda"),
+                walls=walls, wall_width=2, u64_i=u)
+    torch.cuda.synchronize()
+    assert np.array_equal(u.cpu().numpy(), u_o)
+    assert np.array_equal(u32.cpu().numpy(), u_o.astype(np.float32))
+    if walls:
+        un = u.cpu().numpy()
+        assert (un[:3] == 0).all()                   # x low: no-slip (width 2 + ghosts)
+        assert (un[-3:, :, :, 0] == 0).all()         # x high: free-slip, normal component
