@@ -239,6 +239,18 @@ void g2p(const B200::GridArray& u_i, const B200::ParticleMember& c_p,
                 "APIC::g2p");
 }
 
+// APIC::g2p followed by the position update x_p += dt * c_p(0, :) in one
+// pass (collocated, 3 components; positions of sd.x are updated in place).
+template <class Location, class Order>
+void g2pAdvect(const B200::GridArray& u_i, const B200::ParticleMember& c_p,
+               const B200::SplineData<Location, Order>& sd, double dt,
+               const B200::Exec& ex = B200::Exec())
+{
+    B200::check(picasso_apic_g2p_advect(&sd.spline, sd.num_particles(), sd.x.field, u_i.field,
+                                        c_p.field, dt, &ex.exec),
+                "APIC::g2pAdvect");
+}
+
 }  // namespace APIC
 
 namespace PolyPIC {
@@ -278,5 +290,48 @@ inline void inverse(int64_t n, const double* a, double* a_inv, double* det,
 }
 
 }  // namespace LinearAlgebra
+
+namespace B200 {
+
+// Field solve between P2G and G2P (doc/basic/explict_nearly_incompressible_flow.md):
+// u_i = (mu_i + dt f_i) / m_i + dt g, then the wall conditions of `params`.
+// `f_i.field.data == nullptr` means no force.
+inline void gridUpdate(const picasso_mesh& mesh, const GridArray& m_i, const GridArray& mu_i,
+                       const GridArray& f_i, const picasso_grid_update_params& params,
+                       const GridArray& u_i, const Exec& ex = Exec())
+{
+    picasso_grid_field none{};
+    check(picasso_grid_update(&mesh, m_i.field, mu_i.field, f_i.field, &params, u_i.field, none,
+                              &ex.exec),
+          "gridUpdate");
+}
+
+// Many independent APIC problems stepped together (picasso_batch_*); owns the
+// batch handle.
+class Batch {
+  public:
+    Batch(const picasso_batch_instance* instances, int32_t count,
+          picasso_batch_mode mode = PICASSO_BATCH_PHASED)
+    {
+        check(picasso_batch_create(instances, count, mode, &b_), "Batch");
+    }
+    ~Batch() { picasso_batch_destroy(b_); }
+    Batch(const Batch&) = delete;
+    Batch& operator=(const Batch&) = delete;
+    void step(void* stream = nullptr, bool use_graph = true)
+    {
+        check(picasso_batch_step(b_, stream, use_graph ? 1 : 0), "Batch::step");
+    }
+    void stepSequential(void* stream = nullptr)
+    {
+        check(picasso_batch_step_sequential(b_, stream), "Batch::stepSequential");
+    }
+    void status(void* stream = nullptr) { check(picasso_batch_status(b_, stream), "Batch::status"); }
+
+  private:
+    picasso_batch* b_ = nullptr;
+};
+
+}  // namespace B200
 
 }  // namespace Picasso

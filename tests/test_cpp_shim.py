@@ -24,6 +24,41 @@ def test_header_compiles_standalone(tmp_path):
                     "-o", str(tmp_path / "inc")], check=True)
 
 
+def test_header_wrappers_instantiate(tmp_path):
+    """Every wrapper template of the header instantiates and links against
+    the library's exported symbols (nothing is run)."""
+    src = tmp_path / "inst.cpp"
+    src.write_text(r'''
+#include "picasso_b200.hpp"
+using namespace Picasso;
+int main(int argc, char**) {
+    if (argc > 100) {  // never taken: only instantiation and linking are tested
+        picasso_mesh mesh{};
+        double* xd = nullptr; float* mf = nullptr; float* cf = nullptr;
+        int32_t ext[3] = {8, 8, 8};
+        auto x = B200::ParticleMember::aos(xd, 1, 1, 3);
+        auto m = B200::ParticleMember::aos(mf, 1, 1, 1);
+        auto c = B200::ParticleMember::aos(cf, 1, 4, 3);
+        auto u = B200::GridArray::layout_right(cf, ext, 3);
+        auto sd = createSpline(FieldLocation::Node(), InterpolationOrder<2>(), mesh, x);
+        APIC::p2g(m, c, u, u, sd);
+        APIC::g2p(u, c, sd);
+        APIC::g2pAdvect(u, c, sd, 0.1);
+        PolyPIC::g2p(u, c, sd);
+        picasso_grid_update_params prm{};
+        B200::gridUpdate(mesh, u, u, u, prm, u);
+        B200::Batch batch(nullptr, 0);
+        batch.step();
+    }
+    return 0;
+}
+''')
+    lib = os.path.join(ROOT, "picasso_b200")
+    subprocess.run([CXX, "-std=c++14", "-Wall", "-Wextra", "-Werror", "-Wno-unused-parameter",
+                    "-I", INC, str(src), "-L", lib, "-lpicasso_b200", "-Wl,-rpath," + lib, "-o",
+                    str(tmp_path / "inst")], check=True)
+
+
 @pytest.mark.gpu
 def test_shim_reproduces_golden(cuda, tmp_path):
     exe = str(tmp_path / "shim_golden")
