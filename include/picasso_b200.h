@@ -8,7 +8,8 @@
  * batched 3x3 linear algebra used by PolyPIC.
  *
  * Every entry point takes plain pointers, sizes and POD descriptors; device
- * pointers are CUDA device memory on the current device.  All launches are
+ * pointers are CUDA device memory on the current device.  Calls over zero
+ * particles are valid no-ops (their particle pointers may then be NULL).  All launches are
  * asynchronous on the stream in picasso_exec; a returned PICASSO_OK means the
  * arguments were valid and the work was enqueued.  No exceptions cross the ABI.
  *

@@ -62,9 +62,10 @@ picasso_status make_mesh(const picasso_spline* sd, MeshP* mp)
     return PICASSO_OK;
 }
 
-picasso_status validate_pfield(const picasso_particle_field& f, int dtype_a, int dtype_b)
+picasso_status validate_pfield(int64_t n, const picasso_particle_field& f, int dtype_a,
+                               int dtype_b)
 {
-    if (!f.data) return PICASSO_ERR_INVALID_ARGUMENT;
+    if (!f.data && n > 0) return PICASSO_ERR_INVALID_ARGUMENT;
     if (f.dtype != dtype_a && f.dtype != dtype_b) return PICASSO_ERR_INVALID_ARGUMENT;
     if (f.vector_shift < 0) return PICASSO_ERR_INVALID_ARGUMENT;
     if (f.vector_shift < 62 && f.tile_stride < 0) return PICASSO_ERR_INVALID_ARGUMENT;

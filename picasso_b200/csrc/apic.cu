@@ -147,9 +147,9 @@ extern "C" picasso_status picasso_apic_p2g(const picasso_spline* sd, int64_t num
     if (num_particles < 0) return PICASSO_ERR_INVALID_ARGUMENT;
     const int stag = staggered_dim(sd->location);
     if (stag >= 0 ? ncomp != 3 : (ncomp < 1 || ncomp > 3)) return PICASSO_ERR_INVALID_ARGUMENT;
-    if ((st = validate_pfield(x_p, PICASSO_F64))) return st;
-    if ((st = validate_pfield(m_p, PICASSO_F64, PICASSO_F32))) return st;
-    if ((st = validate_pfield(c_p, m_p.dtype))) return st;
+    if ((st = validate_pfield(num_particles, x_p, PICASSO_F64))) return st;
+    if ((st = validate_pfield(num_particles, m_p, PICASSO_F64, PICASSO_F32))) return st;
+    if ((st = validate_pfield(num_particles, c_p, m_p.dtype))) return st;
     if ((st = validate_gfield(m_i, PICASSO_F64, PICASSO_I64_FIXED))) return st;
     if ((st = validate_gfield(mu_i, m_i.dtype))) return st;
     Form form;
@@ -190,9 +190,9 @@ static picasso_status apic_g2p_entry(const picasso_spline* sd, int64_t num_parti
     const int stag = staggered_dim(sd->location);
     if (stag >= 0 ? ncomp != 3 : (ncomp < 1 || ncomp > 3)) return PICASSO_ERR_INVALID_ARGUMENT;
     if (dt && (stag >= 0 || ncomp != 3)) return PICASSO_ERR_INVALID_ARGUMENT;
-    if ((st = validate_pfield(x_p, PICASSO_F64))) return st;
+    if ((st = validate_pfield(num_particles, x_p, PICASSO_F64))) return st;
     if ((st = validate_gfield(u_i, PICASSO_F64, PICASSO_F32))) return st;
-    if ((st = validate_pfield(c_p, u_i.dtype))) return st;
+    if ((st = validate_pfield(num_particles, c_p, u_i.dtype))) return st;
     if (num_particles == 0) return PICASSO_OK;
     const bool f32 = u_i.dtype == PICASSO_F32;
     cudaStream_t s = stream_of(exec);

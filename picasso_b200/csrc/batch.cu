@@ -474,9 +474,9 @@ picasso_status make_instance(const picasso_batch_instance& in, bool f32, BInst* 
         return PICASSO_ERR_INVALID_ARGUMENT;
     const int pt = f32 ? PICASSO_F32 : PICASSO_F64;
     const int gt = f32 ? PICASSO_I64_FIXED : PICASSO_F64;
-    if ((st = validate_pfield(in.x_p, PICASSO_F64))) return st;
-    if ((st = validate_pfield(in.m_p, pt))) return st;
-    if ((st = validate_pfield(in.c_p, pt))) return st;
+    if ((st = validate_pfield(in.num_particles, in.x_p, PICASSO_F64))) return st;
+    if ((st = validate_pfield(in.num_particles, in.m_p, pt))) return st;
+    if ((st = validate_pfield(in.num_particles, in.c_p, pt))) return st;
     if ((st = validate_gfield(in.m_i, gt))) return st;
     if ((st = validate_gfield(in.mu_i, gt))) return st;
     if ((st = validate_gfield(in.u_i, pt))) return st;

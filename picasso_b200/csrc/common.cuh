@@ -144,7 +144,9 @@ inline int staggered_dim(int loc)
 // Validates the mesh / location / order and fills the device parameters.
 picasso_status make_mesh(const picasso_spline* sd, MeshP* mp);
 picasso_status validate_mesh(const picasso_mesh* m);
-picasso_status validate_pfield(const picasso_particle_field& f, int dtype_a, int dtype_b = -1);
+// A member of n particles; null data is accepted when n == 0.
+picasso_status validate_pfield(int64_t n, const picasso_particle_field& f, int dtype_a,
+                               int dtype_b = -1);
 picasso_status validate_gfield(const picasso_grid_field& f, int dtype_a, int dtype_b = -1);
 
 // Knots per dimension and offset of the first knot from floor(x0).

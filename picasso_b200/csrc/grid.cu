@@ -251,8 +251,8 @@ extern "C" picasso_status picasso_advect(const picasso_mesh* mesh, int64_t num_p
     picasso_status st = validate_mesh(mesh);
     if (st) return st;
     if (num_particles < 0) return PICASSO_ERR_INVALID_ARGUMENT;
-    if ((st = validate_pfield(x_p, PICASSO_F64))) return st;
-    if ((st = validate_pfield(c_p, PICASSO_F64, PICASSO_F32))) return st;
+    if ((st = validate_pfield(num_particles, x_p, PICASSO_F64))) return st;
+    if ((st = validate_pfield(num_particles, c_p, PICASSO_F64, PICASSO_F32))) return st;
     if (num_particles == 0) return PICASSO_OK;
     PField x = make_pfield(x_p), c = make_pfield(c_p);
     const Advect a = make_advect(*mesh, dt);

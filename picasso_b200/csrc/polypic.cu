@@ -380,10 +380,10 @@ extern "C" picasso_status picasso_polypic_p2g(const picasso_spline* sd, int64_t 
     int stag, col;
     picasso_status st = polypic_common(sd, num_particles, ncomp, &mp, &stag, &col);
     if (st) return st;
-    if ((st = validate_pfield(x_p, PICASSO_F64))) return st;
-    if ((st = validate_pfield(m_p, PICASSO_F64, PICASSO_F32))) return st;
-    if ((st = validate_pfield(u_p, m_p.dtype))) return st;
-    if ((st = validate_pfield(c_p, m_p.dtype))) return st;
+    if ((st = validate_pfield(num_particles, x_p, PICASSO_F64))) return st;
+    if ((st = validate_pfield(num_particles, m_p, PICASSO_F64, PICASSO_F32))) return st;
+    if ((st = validate_pfield(num_particles, u_p, m_p.dtype))) return st;
+    if ((st = validate_pfield(num_particles, c_p, m_p.dtype))) return st;
     if ((st = validate_gfield(m_i, PICASSO_F64, PICASSO_I64_FIXED))) return st;
     if ((st = validate_gfield(mu_i, m_i.dtype))) return st;
     int form;
@@ -420,9 +420,9 @@ extern "C" picasso_status picasso_polypic_g2p(const picasso_spline* sd, int64_t 
     int stag, col;
     picasso_status st = polypic_common(sd, num_particles, ncomp, &mp, &stag, &col);
     if (st) return st;
-    if ((st = validate_pfield(x_p, PICASSO_F64))) return st;
+    if ((st = validate_pfield(num_particles, x_p, PICASSO_F64))) return st;
     if ((st = validate_gfield(u_i, PICASSO_F64, PICASSO_F32))) return st;
-    if ((st = validate_pfield(c_p, u_i.dtype))) return st;
+    if ((st = validate_pfield(num_particles, c_p, u_i.dtype))) return st;
     if (num_particles == 0) return PICASSO_OK;
     const bool f32 = u_i.dtype == PICASSO_F32;
     cudaStream_t s = stream_of(exec);

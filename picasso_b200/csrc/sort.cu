@@ -382,8 +382,8 @@ extern "C" picasso_status picasso_cell_sort(const picasso_spline* sd, int64_t nu
     SortPlan pl;
     picasso_status st = make_plan(sd, num_particles, tile, &pl);
     if (st) return st;
-    if ((st = validate_pfield(x_p, PICASSO_F64))) return st;
-    if (!key || !perm || !tile_offset || !tile_items || !workspace ||
+    if ((st = validate_pfield(num_particles, x_p, PICASSO_F64))) return st;
+    if ((num_particles > 0 && (!key || !perm)) || !tile_offset || !tile_items || !workspace ||
         workspace_bytes < pl.bytes || chunk < 32)
         return PICASSO_ERR_INVALID_ARGUMENT;
     if (reinterpret_cast<uintptr_t>(workspace) % 256) return PICASSO_ERR_INVALID_ARGUMENT;
@@ -457,11 +457,12 @@ extern "C" picasso_status picasso_permute(int64_t num_particles, int32_t ncomp,
                                           const uint32_t* perm, picasso_particle_field src,
                                           picasso_particle_field dst, const picasso_exec* exec)
 {
-    if (num_particles < 0 || ncomp < 1 || !perm) return PICASSO_ERR_INVALID_ARGUMENT;
+    if (num_particles < 0 || ncomp < 1 || (num_particles > 0 && !perm))
+        return PICASSO_ERR_INVALID_ARGUMENT;
     picasso_status st;
-    if ((st = validate_pfield(src, PICASSO_F64, PICASSO_F32))) return st;
-    if ((st = validate_pfield(dst, src.dtype))) return st;
-    if (src.data == dst.data) return PICASSO_ERR_INVALID_ARGUMENT;
+    if ((st = validate_pfield(num_particles, src, PICASSO_F64, PICASSO_F32))) return st;
+    if ((st = validate_pfield(num_particles, dst, src.dtype))) return st;
+    if (num_particles > 0 && src.data == dst.data) return PICASSO_ERR_INVALID_ARGUMENT;
     if (num_particles == 0) return PICASSO_OK;
     cudaStream_t s = stream_of(exec);
     const int64_t esize = src.dtype == PICASSO_F64 ? 8 : 4;
