@@ -51,18 +51,26 @@ __global__ void __launch_bounds__(kG2PThreads) g2p_tiled_kernel(G2PArgs A, int64
 // of a millisecond, so results are cached per (tile nodes, K, F) for callers
 // that alternate between tile shapes (batches of meshes).
 struct StrideKey {
-    int NT[3], K, F;
+    int NT[3], K, F, split;
     bool operator==(const StrideKey& o) const
     {
-        return NT[0] == o.NT[0] && NT[1] == o.NT[1] && NT[2] == o.NT[2] && K == o.K && F == o.F;
+        return NT[0] == o.NT[0] && NT[1] == o.NT[1] && NT[2] == o.NT[2] && K == o.K &&
+               F == o.F && split == o.split;
     }
 };
 
+// Tile strides (SJ, SI, P) that spread the tile offsets of one merge round
+// (32 staged values added by 32 lanes) over as many shared-memory banks as
+// possible; the smallest tile among equals.  `split`: the staging of the
+// i-plane split (F fields of K^2 nodes per lane, whose k-plane merges are
+// counted as well).
 static void search_strides(const StrideKey& key, int* SJ, int* SI, int* P)
 {
     const int* NT = key.NT;
     const int K = key.K, F = key.F;
-    const int KKK = K * K * K, FS = (KKK + 3) & ~3, SV = F * FS, R = (SV + 31) / 32;
+    const int NL = key.split ? K * K : K * K * K, FS = (NL + 3) & ~3, SV = F * FS;
+    const int R = (SV + 31) / 32;
+    const int ROWS = NL / K, PV = F * ROWS, RP = key.split ? (PV + 31) / 32 : 0;
     int best = -1, bsj = NT[2], bsi = NT[1] * NT[2], bp = NT[0] * NT[1] * NT[2];
     long best_size = 0;
     for (int sj = NT[2]; sj < NT[2] + 8; ++sj)
@@ -73,9 +81,21 @@ static void search_strides(const StrideKey& key, int* SJ, int* SI, int* P)
                     unsigned banks = 0;
                     for (int lane = 0; lane < 32; ++lane) {
                         const int v = lane + 32 * r, f = v / FS, nn = v % FS;
-                        if (v >= SV || nn >= KKK) continue;
+                        if (v >= SV || nn >= NL) continue;
                         const int a = nn / (K * K), b = (nn / K) % K, c = nn % K;
                         const int off = f * pp + a * si + b * sj + c;
+                        const unsigned bit = 1u << (off & 31);
+                        if (!(banks & bit)) ++distinct;
+                        banks |= bit;
+                    }
+                }
+                for (int r = 0; r < RP; ++r) {
+                    unsigned banks = 0;
+                    for (int lane = 0; lane < 32; ++lane) {
+                        const int v = lane + 32 * r;
+                        if (v >= PV) continue;
+                        const int ij = v % ROWS;
+                        const int off = (v / ROWS) * pp + (ij / K) * si + (ij % K) * sj;
                         const unsigned bit = 1u << (off & 31);
                         if (!(banks & bit)) ++distinct;
                         banks |= bit;
@@ -95,14 +115,14 @@ static void search_strides(const StrideKey& key, int* SJ, int* SI, int* P)
     *P = bp;
 }
 
-static void choose_strides(const int NT[3], int K, int F, int* SJ, int* SI, int* P)
+static void choose_strides(const int NT[3], int K, int F, int split, int* SJ, int* SI, int* P)
 {
     constexpr int kSlots = 64;
     static std::mutex mu;
     static StrideKey keys[kSlots];
     static int vals[kSlots][3];
     static int used = 0, next = 0;
-    const StrideKey key{{NT[0], NT[1], NT[2]}, K, F};
+    const StrideKey key{{NT[0], NT[1], NT[2]}, K, F, split};
     {
         std::lock_guard<std::mutex> lock(mu);
         for (int i = 0; i < used; ++i)
@@ -121,6 +141,10 @@ static void choose_strides(const int NT[3], int K, int F, int* SJ, int* SI, int*
     vals[slot][1] = *SI;
     vals[slot][2] = *P;
 }
+
+static_assert(P2GCfg<3, 4>::ISPLIT && !P2GCfg<2, 4>::ISPLIT && !P2GCfg<1, 4>::ISPLIT &&
+                  !P2GCfg<1, 2>::ISPLIT,
+              "make_tilep's stride choice follows the accumulator split");
 
 int default_lpp(int order) { return order == 3 ? 4 : 1; }
 
@@ -149,7 +173,9 @@ bool make_tilep(const MeshP& mp, int order, const picasso_bins& bins, TileP* tp,
     }
     tp->nodes = tp->NT[0] * tp->NT[1] * tp->NT[2];
     if (lpp > 0) {
-        choose_strides(tp->NT, K, 4 / lpp, &tp->SJ, &tp->SI, &tp->P);
+        // the accumulator split of p2g_item (P2GCfg::ISPLIT, F)
+        const int split = order == 3 && lpp == 4;
+        choose_strides(tp->NT, K, split ? 4 : 4 / lpp, split, &tp->SJ, &tp->SI, &tp->P);
     } else {
         tp->SJ = tp->NT[2];
         tp->SI = tp->NT[1] * tp->NT[2];

@@ -181,17 +181,25 @@ template <int ORDER, int LPP>
 struct P2GCfg {
     static constexpr int K = SplineTraits<ORDER>::K;
     static constexpr int KKK = K * K * K;
-    static constexpr int FS = (KKK + 3) & ~3;  // staged floats per field
-    static constexpr int F = 4 / LPP;          // fields per lane
-    static constexpr int RUNS = 32 / LPP;      // runs per warp
-    static constexpr int SV = F * FS;          // staged values per lane
+    // Cubic stencils with 4 lanes per particle split the stencil by its
+    // i-planes (lane h sums all four fields of the 16 nodes (h, j, k)); the
+    // other splits are by field (lane h sums fields h F .. h F + F - 1 of all
+    // K^3 nodes).  The plane split needs one x-weight per lane and shares the
+    // affine products of a (j, k) node between the three momentum fields.
+    static constexpr bool ISPLIT = ORDER == 3 && LPP == 4;
+    static constexpr int NL = ISPLIT ? K * K : KKK;  // nodes per lane
+    static constexpr int ROWS = NL / K;              // k-rows per lane
+    static constexpr int FS = (NL + 3) & ~3;         // staged floats per field
+    static constexpr int F = ISPLIT ? 4 : 4 / LPP;   // fields per lane
+    static constexpr int RUNS = 32 / LPP;            // runs per warp
+    static constexpr int SV = F * FS;                // staged values per lane
     // staging stride: a multiple of 4 floats whose quarter is odd keeps the
     // float4 stores of 8 staged lanes on distinct banks
     static constexpr int SS = ((SV / 4) % 2 == 0) ? SV + 4 : SV;
     static constexpr int R = (SV + 31) / 32;  // merge rounds per staged lane
     // k-plane merges (a lane's bin advanced by one along k): the K^2 nodes of
     // the stencil's first k-plane, F fields, packed
-    static constexpr int PV = F * K * K;
+    static constexpr int PV = F * ROWS;
     static constexpr int PV4 = (PV + 3) & ~3;
     static constexpr int PS = ((PV4 / 4) % 2 == 0) ? PV4 + 4 : PV4;
     static constexpr int RP = (PV + 31) / 32;
@@ -202,8 +210,10 @@ struct P2GCfg {
     // ring depth: records of DEPTH - 1 particles are in flight per run; the
     // warps with fewer runs (more lanes per particle) need more to keep the
     // same bytes in flight.  Deeper rings cost shared memory, which costs
-    // warps (measured: depth 4 fastest for one lane per particle).
-    static constexpr int DEPTH = LPP == 1 ? 4 : (LPP == 2 ? 8 : 10);
+    // warps (measured: depth 4 fastest for one lane per particle, and for
+    // cubic stencils, whose ~600 instructions per lane and particle hide the
+    // loads: 256^3 8 ppc, tile (4, 4, 8): depth 4 14.6 ms, 6 14.7, 10 15.7).
+    static constexpr int DEPTH = LPP == 1 ? 4 : (LPP == 2 ? 8 : (ORDER == 3 ? 4 : 10));
     static constexpr int STAGE_OFF = DEPTH * RING;
     static constexpr int TILE_OFF = STAGE_OFF + kStageLanes * SS;
     static_assert(LPP == 1 || LPP == 2 || LPP == 4, "1, 2 or 4 lanes per particle");
@@ -226,21 +236,51 @@ __host__ __device__ constexpr int p2g_warp_floats(int P)
 template <int ORDER, int LPP>
 struct P2GAcc {
     using C = P2GCfg<ORDER, LPP>;
-    float acc[C::F][C::KKK];
+    float acc[C::F][C::NL];
 
     __device__ __forceinline__ void zero()
     {
 #pragma unroll
         for (int f = 0; f < C::F; ++f)
 #pragma unroll
-            for (int n = 0; n < C::KKK; ++n) acc[f][n] = 0.f;
+            for (int n = 0; n < C::NL; ++n) acc[f][n] = 0.f;
     }
 
+    // h: the lane's share of the particle (its i-plane when C::ISPLIT)
     __device__ __forceinline__ void add(const Spline1D<ORDER, float> sp[3], float mass,
-                                        const float co[C::F][4])
+                                        const float co[C::F][4], int h)
     {
         constexpr int K = C::K;
-        if (ORDER >= 2) {
+        if constexpr (C::ISPLIT) {
+            // node (h, j, k): w = wx_h wy_j wz_k m, field g = 1..3 receives
+            // w (c0 + cx dist_h + cy dist_j + cz dist_k), the mass w
+            float wx = 0.f, dx = 0.f;
+#pragma unroll
+            for (int i = 0; i < K; ++i)
+                if (i == h) {
+                    wx = sp[0].w[i];
+                    dx = sp[0].d[i];
+                }
+            float e[3];
+#pragma unroll
+            for (int f = 1; f < 4; ++f) e[f - 1] = co[f][0] + co[f][1] * dx;
+#pragma unroll
+            for (int j = 0; j < K; ++j) {
+                const float wij = wx * sp[1].w[j] * mass;
+                float pij[3];
+#pragma unroll
+                for (int f = 1; f < 4; ++f) pij[f - 1] = e[f - 1] + co[f][2] * sp[1].d[j];
+#pragma unroll
+                for (int k = 0; k < K; ++k) {
+                    const int n = j * K + k;
+                    const float w = wij * sp[2].w[k];
+                    acc[0][n] += w;
+#pragma unroll
+                    for (int f = 1; f < 4; ++f)
+                        acc[f][n] += w * (pij[f - 1] + co[f][3] * sp[2].d[k]);
+                }
+            }
+        } else if (ORDER >= 2) {
 #pragma unroll
             for (int i = 0; i < K; ++i)
 #pragma unroll
@@ -292,20 +332,20 @@ struct P2GAcc {
 #pragma unroll
             for (int q = 0; q < C::FS / 4; ++q) {
                 float4 v;
-                v.x = (4 * q + 0 < C::KKK) ? acc[f][4 * q + 0] : 0.f;
-                v.y = (4 * q + 1 < C::KKK) ? acc[f][4 * q + 1] : 0.f;
-                v.z = (4 * q + 2 < C::KKK) ? acc[f][4 * q + 2] : 0.f;
-                v.w = (4 * q + 3 < C::KKK) ? acc[f][4 * q + 3] : 0.f;
+                v.x = (4 * q + 0 < C::NL) ? acc[f][4 * q + 0] : 0.f;
+                v.y = (4 * q + 1 < C::NL) ? acc[f][4 * q + 1] : 0.f;
+                v.z = (4 * q + 2 < C::NL) ? acc[f][4 * q + 2] : 0.f;
+                v.w = (4 * q + 3 < C::NL) ? acc[f][4 * q + 3] : 0.f;
                 *reinterpret_cast<float4*>(st + f * C::FS + 4 * q) = v;
             }
     }
 
-    // value v of the first k-plane: field v / K^2, node (i, j, 0) with
-    // i * K + j = v % K^2
+    // value v of the first k-plane: field v / ROWS, k-row v % ROWS (the row
+    // (i, j) with i * K + j = v % ROWS, or (h, j) with j = v % ROWS for the
+    // plane split), its node k = 0
     __device__ __forceinline__ float plane_value(int v) const
     {
-        constexpr int K = C::K;
-        return acc[v / (K * K)][(v % (K * K)) * K];
+        return acc[v / C::ROWS][(v % C::ROWS) * C::K];
     }
 
     // st[v] <- plane_value(v) with 16-byte stores.
@@ -330,7 +370,7 @@ struct P2GAcc {
 #pragma unroll
         for (int f = 0; f < C::F; ++f)
 #pragma unroll
-            for (int ij = 0; ij < K * K; ++ij) {
+            for (int ij = 0; ij < C::ROWS; ++ij) {
 #pragma unroll
                 for (int k = 0; k + 1 < K; ++k) acc[f][ij * K + k] = acc[f][ij * K + k + 1];
                 acc[f][ij * K + K - 1] = 0.f;
@@ -339,27 +379,28 @@ struct P2GAcc {
 };
 
 // Merge plan of one lane: staged value v = lane + 32 r of a staged lane that
-// handles fields hh F .. hh F + F - 1 lands at tile offset
-// moff[r] + hh * fstride from the stencil start.
+// handles fields hh F .. hh F + F - 1 (plane split: i-plane hh) lands at tile
+// offset moff[r] + hh * fstride from the stencil start.
 template <int ORDER, int LPP>
 struct MergePlan {
     using C = P2GCfg<ORDER, LPP>;
     int moff[C::R];
     int poff[C::RP];  // the same for the values of a k-plane stage
-    int fstride;      // F * P
+    int fstride;      // F * P (plane split: SI)
     unsigned valid;   // bit r: value lane + 32 r exists
     unsigned pvalid;
     __device__ __forceinline__ void init(const TileP& tp, int lane)
     {
         constexpr int K = C::K;
         valid = 0;
-        fstride = C::F * tp.P;
+        // the plane split offsets a staged lane's values by its i-plane
+        fstride = C::ISPLIT ? tp.SI : C::F * tp.P;
 #pragma unroll
         for (int r = 0; r < C::R; ++r) {
             const int v = lane + 32 * r;
             const int fs = v / C::FS, nn = v - (v / C::FS) * C::FS;
             moff[r] = 0;
-            if (v < C::SV && nn < C::KKK) {
+            if (v < C::SV && nn < C::NL) {
                 const int a = nn / (K * K), b = (nn / K) % K, c = nn % K;
                 moff[r] = fs * tp.P + a * tp.SI + b * tp.SJ + c;
                 valid |= 1u << r;
@@ -371,7 +412,7 @@ struct MergePlan {
             const int v = lane + 32 * r;
             poff[r] = 0;
             if (v < C::PV) {
-                const int fs = v / (K * K), ij = v % (K * K);
+                const int fs = v / C::ROWS, ij = v % C::ROWS;
                 poff[r] = fs * tp.P + (ij / K) * tp.SI + (ij % K) * tp.SJ;
                 pvalid |= 1u << r;
             }
@@ -542,7 +583,7 @@ __device__ void p2g_item(const P2GArgs& A, int64_t t, int64_t a, int64_t b, floa
         mass = sl[C::RING_M + run];
 #pragma unroll
         for (int f = 0; f < C::F; ++f) {
-            const int g = h * C::F + f;  // global field
+            const int g = C::ISPLIT ? f : h * C::F + f;  // global field
             if (g == 0) {
                 co[f][0] = 1.f;
                 co[f][1] = co[f][2] = co[f][3] = 0.f;
@@ -590,7 +631,7 @@ __device__ void p2g_item(const P2GArgs& A, int64_t t, int64_t a, int64_t b, floa
             }
             float co[C::F][4], mass;
             coefficients(s, co, mass);
-            acc.add(P.sp, mass, co);
+            acc.add(P.sp, mass, co, h);
         }
     }
     cp_async_wait<0>();
