@@ -470,10 +470,12 @@ def run_ours(args):
 # ---------------------------------------------------------------------------
 def run_advect(args, peak):
     """256^3 periodic grid, 8 ppc uniform, cubic B-spline, dt = 0.1 dx: every
-    step zeroes the grid, P2G, velocity update, G2P fused with the position
-    update, then re-sorts the particles by cell and permutes every member.
-    FP64 plain form (the reference's arithmetic) and FP32 precision form
-    (tiled kernels); both forms start from the same particles."""
+    step re-sorts the particles by cell and permutes every member, zeroes the
+    grid, P2G, velocity update, then G2P fused with the position update, which
+    also emits the moved particles' sort keys for the next step's sort (the
+    first sort starts from the positions).  FP64 plain form (the reference's
+    arithmetic) and FP32 precision form (tiled kernels); both forms start from
+    the same particles."""
     import torch
 
     import picasso_b200 as pb
@@ -487,7 +489,8 @@ def run_advect(args, peak):
     dt = 0.1 / g
     seed = 1001
     res = {"workload": "cubic APIC, %d^3 periodic, 8 ppc uniform, dt = 0.1 dx, per step: "
-                       "fill, P2G, velocity, G2P + advection, cell re-sort + permute" % g,
+                       "cell re-sort (from the keys the previous G2P emitted) + permute, fill, P2G, "
+                       "velocity, G2P + advection + sort keys" % g,
            "steps": args.adv_steps, "tile": list(args.adv_tile)}
     names = ["sort", "permute", "fill", "p2g", "velocity", "g2p_advect"]
     for form in ("fp64", "fp32"):
@@ -507,7 +510,9 @@ def run_advect(args, peak):
             acc = torch.zeros(ext + (4,), dtype=torch.float64, device="cuda")
             gm, gmu, fill = acc[..., 0], acc[..., 1:], acc
             u = torch.zeros(ext + (3,), dtype=torch.float64, device="cuda")
-        state = {"x": x, "m": m, "c": c}
+        state = {"x": x, "m": m, "c": c, "keys": None}
+        keybuf = torch.empty(n, dtype=torch.int32, device="cuda")
+        tile = tuple(args.adv_tile)
 
         def step(ev=None):
             def mark(i):
@@ -515,8 +520,8 @@ def run_advect(args, peak):
                     ev[i].record()
             mark(0)
             sd0 = pb.create_spline(loc, 3, mesh, state["x"])
-            _, perm, bins = pb.cell_sort(sd0, tuple(args.adv_tile), chunk=4096,
-                                         p2g_lanes=4 if f32 else 0)
+            _, perm, bins = pb.cell_sort(sd0, tile, chunk=4096, p2g_lanes=4 if f32 else 0,
+                                         keys=state["keys"])
             mark(1)
             state["x"], state["m"], state["c"] = pb.permute_members(
                 perm, state["x"], state["m"], state["c"])
@@ -528,7 +533,8 @@ def run_advect(args, peak):
             mark(4)
             pb.grid_velocity(desc, gm, gmu, u, 1e-12)
             mark(5)
-            pb.APIC.g2p_advect(u, state["c"], sd, dt, bins=bins)
+            state["keys"] = pb.APIC.g2p_advect(u, state["c"], sd, dt, bins=bins, key_tile=tile,
+                                               keys_out=keybuf)
             mark(6)
 
         step()
@@ -550,7 +556,7 @@ def run_advect(args, peak):
                      "transfer_ms": per["fill"] + per["p2g"] + per["velocity"]
                      + per["g2p_advect"], "kernels_ms": per,
                      "positions_in_box": bool(float(xs.min()) >= 0.0 and float(xs.max()) < 1.0)}
-        del state, x, m, c, acc, u
+        del state, x, m, c, acc, u, keybuf
         torch.cuda.synchronize()
         torch.cuda.empty_cache()
     res["speedup_fp32_vs_fp64"] = res["fp64"]["ms_per_step"] / res["fp32"]["ms_per_step"]

@@ -144,9 +144,10 @@ typedef struct picasso_bins {
     int32_t location;            /* picasso_location the bins were built for */
     int32_t chunk;               /* particles per work item */
     int32_t p2g_lanes;           /* lanes per particle of the tiled P2G: 1, 2 or
-                                    4 for orders 1-2, 4 for order 3 (the 4 grid
-                                    fields are split between them); 0 = the
-                                    library's choice; set to 0 by the sort */
+                                    4 for orders 1-2 (the 4 grid fields are
+                                    split between them), 4 for order 3 (one
+                                    stencil i-plane each); 0 = the library's
+                                    choice; set to 0 by the sort */
     const int64_t* tile_offset;  /* device, num_tiles_total + 1 particle offsets */
     const uint32_t* tile_items;  /* device, num_tiles_total + 1: first work item
                                     of each tile (exclusive prefix of
@@ -300,6 +301,21 @@ PICASSO_API picasso_status picasso_apic_g2p_advect(const picasso_spline* sd,
                                                    picasso_particle_field c_p, double dt,
                                                    const picasso_exec* exec);
 
+/* picasso_apic_g2p_advect that also writes, for every moved particle p,
+ * key_out[p] = its sort key for bins of the given tile shape (the key
+ * picasso_cell_sort defines, computed from the new position with the same
+ * arithmetic), so that the next step's sort can start from the keys
+ * (picasso_cell_sort_keys) instead of re-reading the positions.  key_out is
+ * indexed like the particles (device, num_particles entries).  No reference
+ * counterpart (Picasso has no sort). */
+PICASSO_API picasso_status picasso_apic_g2p_advect_keys(const picasso_spline* sd,
+                                                        int64_t num_particles,
+                                                        picasso_particle_field x_p,
+                                                        picasso_grid_field u_i,
+                                                        picasso_particle_field c_p, double dt,
+                                                        const int32_t tile[3], uint32_t* key_out,
+                                                        const picasso_exec* exec);
+
 /* ------------------------------------------------------------------------ */
 /* Particle cell-sort                                                       */
 /* ------------------------------------------------------------------------ */
@@ -330,6 +346,21 @@ PICASSO_API picasso_status picasso_cell_sort(const picasso_spline* sd, int64_t n
                                  int64_t* tile_offset, uint32_t* tile_items,
                                  void* workspace, int64_t workspace_bytes,
                                  picasso_bins* bins_out, const picasso_exec* exec);
+
+/* picasso_cell_sort from keys the caller already has: key_in[p] (device) is
+ * the sort key of particle p as picasso_cell_sort defines it, e.g. written by
+ * picasso_apic_g2p_advect_keys for the same spline and tile shape.  Keys
+ * above num_tiles * tile volume count as that value (outside the mesh).
+ * Same outputs as picasso_cell_sort on the positions the keys came from.
+ * key_in must not overlap key, perm or the workspace; it is not modified.
+ * No reference counterpart. */
+PICASSO_API picasso_status picasso_cell_sort_keys(const picasso_spline* sd, int64_t num_particles,
+                                                  const uint32_t* key_in, const int32_t tile[3],
+                                                  int32_t chunk, uint32_t* key, uint32_t* perm,
+                                                  int64_t* tile_offset, uint32_t* tile_items,
+                                                  void* workspace, int64_t workspace_bytes,
+                                                  picasso_bins* bins_out,
+                                                  const picasso_exec* exec);
 
 /* picasso_cell_sort for callers that cannot allocate device memory when they
  * sort (an application that gives all GPU memory to its own pool at start-up,

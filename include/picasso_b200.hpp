@@ -251,6 +251,19 @@ void g2pAdvect(const B200::GridArray& u_i, const B200::ParticleMember& c_p,
                 "APIC::g2pAdvect");
 }
 
+// g2pAdvect that also writes key_out[p] (device), the cell-sort key of every
+// moved particle for bins of shape `tile`: the input of
+// picasso_cell_sort_keys for the next step.
+template <class Location, class Order>
+void g2pAdvect(const B200::GridArray& u_i, const B200::ParticleMember& c_p,
+               const B200::SplineData<Location, Order>& sd, double dt, const int32_t tile[3],
+               uint32_t* key_out, const B200::Exec& ex = B200::Exec())
+{
+    B200::check(picasso_apic_g2p_advect_keys(&sd.spline, sd.num_particles(), sd.x.field,
+                                             u_i.field, c_p.field, dt, tile, key_out, &ex.exec),
+                "APIC::g2pAdvect");
+}
+
 }  // namespace APIC
 
 namespace PolyPIC {

@@ -119,10 +119,17 @@ SIGNATURES = [
     ("picasso_apic_g2p_advect", C.c_int,
      [C.POINTER(Spline), C.c_int64, ParticleField, GridField, ParticleField, C.c_double,
       C.POINTER(Exec)]),
+    ("picasso_apic_g2p_advect_keys", C.c_int,
+     [C.POINTER(Spline), C.c_int64, ParticleField, GridField, ParticleField, C.c_double,
+      C.POINTER(C.c_int32), C.c_void_p, C.POINTER(Exec)]),
     ("picasso_cell_sort_workspace", C.c_int,
      [C.POINTER(Spline), C.c_int64, C.POINTER(C.c_int32), C.POINTER(C.c_int64)]),
     ("picasso_cell_sort", C.c_int,
      [C.POINTER(Spline), C.c_int64, ParticleField, C.POINTER(C.c_int32), C.c_int32, C.c_void_p,
+      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.POINTER(Bins),
+      C.POINTER(Exec)]),
+    ("picasso_cell_sort_keys", C.c_int,
+     [C.POINTER(Spline), C.c_int64, C.c_void_p, C.POINTER(C.c_int32), C.c_int32, C.c_void_p,
       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.POINTER(Bins),
       C.POINTER(Exec)]),
     ("picasso_cell_sort_static", C.c_int,

@@ -315,16 +315,33 @@ class APIC:
                                       C.byref(ex.desc)), "APIC::g2p")
 
     @staticmethod
-    def g2p_advect(u_i, c_p, sd, dt, stream=None, error_count=None, bins=None):
+    def g2p_advect(u_i, c_p, sd, dt, stream=None, error_count=None, bins=None, key_tile=None,
+                   keys_out=None):
         """APIC::g2p followed by the position update x_p += dt * c_p(0, :)
         (FP64, periodic wrap) in one pass; collocated, 3 components.  The
-        spline's positions sd.x are updated in place."""
+        spline's positions sd.x are updated in place.  With key_tile (a tile
+        shape) it also returns the sort key of every moved particle (int32
+        tensor of uint32 values, written into keys_out if given), the input of
+        cell_sort(..., keys=...) for the next step."""
         _check_grid_extent(u_i, sd.desc.mesh)
         ex = _exec(stream, error_count, bins)
-        check(_lib().picasso_apic_g2p_advect(C.byref(sd.desc), sd.num_particles,
-                                             particle_field(sd.x), grid_field(u_i),
-                                             particle_field(c_p), float(dt), C.byref(ex.desc)),
-              "APIC::g2p_advect")
+        if key_tile is None:
+            check(_lib().picasso_apic_g2p_advect(C.byref(sd.desc), sd.num_particles,
+                                                 particle_field(sd.x), grid_field(u_i),
+                                                 particle_field(c_p), float(dt),
+                                                 C.byref(ex.desc)), "APIC::g2p_advect")
+            return None
+        n = sd.num_particles
+        if keys_out is None:
+            keys_out = torch.empty(max(n, 1), dtype=torch.int32, device=sd.x.device)
+        elif keys_out.dtype != torch.int32 or keys_out.numel() < n or not keys_out.is_contiguous():
+            raise ValueError("keys_out: contiguous int32 tensor of at least %d entries" % n)
+        t3 = (C.c_int32 * 3)(*key_tile)
+        check(_lib().picasso_apic_g2p_advect_keys(C.byref(sd.desc), n, particle_field(sd.x),
+                                                  grid_field(u_i), particle_field(c_p),
+                                                  float(dt), t3, keys_out.data_ptr(),
+                                                  C.byref(ex.desc)), "APIC::g2p_advect")
+        return keys_out[:n]
 
 
 class PolyPIC:
@@ -426,12 +443,15 @@ class Bins:
         return self.desc.num_tiles[0] * self.desc.num_tiles[1] * self.desc.num_tiles[2]
 
 
-def cell_sort(sd, tile=(4, 8, 8), chunk=4096, stream=None, workspace=None, p2g_lanes=0):
+def cell_sort(sd, tile=(4, 8, 8), chunk=4096, stream=None, workspace=None, p2g_lanes=0,
+              keys=None):
     """Stable sort of the spline's particles by (tile, bin).  Returns
     (key, perm, bins): keys and permutation as int32 tensors holding uint32
     values, and the Bins to pass to the transfers once the particle members
     have been permuted (see permute / permute_members).  `p2g_lanes` (1, 2, 4;
-    0 = library choice) is the tiled P2G's lanes per particle."""
+    0 = library choice) is the tiled P2G's lanes per particle.  `keys`: the
+    particles' keys for this tile shape as APIC.g2p_advect(key_tile=tile)
+    returned them; the sort then starts from them instead of the positions."""
     lib = _lib()
     n = sd.num_particles
     t3 = (C.c_int32 * 3)(*tile)
@@ -452,10 +472,20 @@ def cell_sort(sd, tile=(4, 8, 8), chunk=4096, stream=None, workspace=None, p2g_l
     tile_items = torch.empty(nt + 1, dtype=torch.int32, device=dev)
     bins = _abi.Bins()
     ex = _exec(stream, None, None)
-    check(lib.picasso_cell_sort(C.byref(sd.desc), n, particle_field(sd.x), t3, int(chunk),
-                                key.data_ptr(), perm.data_ptr(), tile_offset.data_ptr(),
-                                tile_items.data_ptr(), workspace.data_ptr(), workspace.numel(),
-                                C.byref(bins), C.byref(ex.desc)), "cell_sort")
+    if keys is not None:
+        if keys.dtype != torch.int32 or keys.numel() < n or not keys.is_contiguous():
+            raise ValueError("keys: contiguous int32 tensor of at least %d entries" % n)
+        check(lib.picasso_cell_sort_keys(C.byref(sd.desc), n, keys.data_ptr(), t3, int(chunk),
+                                         key.data_ptr(), perm.data_ptr(), tile_offset.data_ptr(),
+                                         tile_items.data_ptr(), workspace.data_ptr(),
+                                         workspace.numel(), C.byref(bins), C.byref(ex.desc)),
+              "cell_sort")
+    else:
+        check(lib.picasso_cell_sort(C.byref(sd.desc), n, particle_field(sd.x), t3, int(chunk),
+                                    key.data_ptr(), perm.data_ptr(), tile_offset.data_ptr(),
+                                    tile_items.data_ptr(), workspace.data_ptr(),
+                                    workspace.numel(), C.byref(bins), C.byref(ex.desc)),
+              "cell_sort")
     bins.p2g_lanes = int(p2g_lanes)
     return key[:n], perm[:n], Bins(bins, tile_offset, tile_items)
 

@@ -178,10 +178,14 @@ extern "C" picasso_status picasso_apic_p2g(const picasso_spline* sd, int64_t num
 }
 
 // G2P, and with dt != nullptr the position update x += dt u_p after it.
+// dt != nullptr: G2P with advection; key_out != nullptr: it also writes the
+// sort key of every moved particle for bins of the given tile shape.
 static picasso_status apic_g2p_entry(const picasso_spline* sd, int64_t num_particles,
                                      int32_t ncomp, picasso_particle_field x_p,
                                      picasso_grid_field u_i, picasso_particle_field c_p,
-                                     const double* dt, const picasso_exec* exec)
+                                     const double* dt, const picasso_exec* exec,
+                                     const int32_t* key_tile = nullptr,
+                                     uint32_t* key_out = nullptr)
 {
     MeshP mp;
     picasso_status st = make_mesh(sd, &mp);
@@ -193,6 +197,12 @@ static picasso_status apic_g2p_entry(const picasso_spline* sd, int64_t num_parti
     if ((st = validate_pfield(num_particles, x_p, PICASSO_F64))) return st;
     if ((st = validate_gfield(u_i, PICASSO_F64, PICASSO_F32))) return st;
     if ((st = validate_pfield(num_particles, c_p, u_i.dtype))) return st;
+    BinP bins;
+    if (key_tile) {
+        int64_t ntiles = 0;
+        if ((st = make_binp(sd, key_tile, &bins, &ntiles))) return st;
+        if (num_particles > 0 && !key_out) return PICASSO_ERR_INVALID_ARGUMENT;
+    }
     if (num_particles == 0) return PICASSO_OK;
     const bool f32 = u_i.dtype == PICASSO_F32;
     cudaStream_t s = stream_of(exec);
@@ -201,6 +211,10 @@ static picasso_status apic_g2p_entry(const picasso_spline* sd, int64_t num_parti
     GField u = make_gfield(u_i);
     Advect adv;
     if (dt) adv = make_advect(sd->mesh, *dt);
+    if (dt && key_tile) {
+        adv.key_out = key_out;
+        adv.bins = bins;
+    }
     const Advect* ap = dt ? &adv : nullptr;
     if (exec && exec->bins) {
         if (exec->bins->order != sd->order || exec->bins->location != sd->location)
@@ -231,4 +245,16 @@ extern "C" picasso_status picasso_apic_g2p_advect(const picasso_spline* sd,
                                                   const picasso_exec* exec)
 {
     return apic_g2p_entry(sd, num_particles, 3, x_p, u_i, c_p, &dt, exec);
+}
+
+extern "C" picasso_status picasso_apic_g2p_advect_keys(const picasso_spline* sd,
+                                                       int64_t num_particles,
+                                                       picasso_particle_field x_p,
+                                                       picasso_grid_field u_i,
+                                                       picasso_particle_field c_p, double dt,
+                                                       const int32_t tile[3], uint32_t* key_out,
+                                                       const picasso_exec* exec)
+{
+    if (!tile) return PICASSO_ERR_INVALID_ARGUMENT;
+    return apic_g2p_entry(sd, num_particles, 3, x_p, u_i, c_p, &dt, exec, tile, key_out);
 }

@@ -3,6 +3,7 @@
 // momentum-to-velocity update with the near-empty-node threshold.
 #pragma once
 
+#include "binkey.cuh"
 #include "common.cuh"
 
 namespace pb {
@@ -108,12 +109,17 @@ struct Advect {
     int periodic[3];
     double lo[3];   // coordinate of the owned box's low face
     double len[3];  // owned box length
+    // optional: key_out[p] = sort key (bins) of the moved particle p, the key
+    // the cell sort would compute from the new position
+    uint32_t* key_out;
+    BinP bins;
 };
 
 inline Advect make_advect(const picasso_mesh& m, double dt)
 {
-    Advect a;
+    Advect a{};
     a.dt = dt;
+    a.key_out = nullptr;
     for (int d = 0; d < 3; ++d) {
         a.periodic[d] = m.periodic[d] != 0;
         a.lo[d] = m.low_corner[d] + m.own_begin[d] * m.cell_size[d];
@@ -130,6 +136,21 @@ __device__ __forceinline__ double advect_coord(const Advect& a, int d, double x,
         else if (xn >= a.lo[d] + a.len[d]) xn -= a.len[d];
     }
     return xn;
+}
+
+// Moves particle p (x_p += dt u_p, wrapped) and emits its new sort key when
+// asked for; xp: the old position, u: the stored velocity.
+template <class XStore>
+__device__ __forceinline__ void advect_particle(const Advect& a, int64_t p, const double xp[3],
+                                                const double u[3], XStore&& store)
+{
+    double xn[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        xn[d] = advect_coord(a, d, xp[d], u[d]);
+        store(d, xn[d]);
+    }
+    if (a.key_out) a.key_out[p] = particle_key(a.bins, xn);
 }
 
 }  // namespace pb

@@ -204,9 +204,9 @@ __device__ __forceinline__ void apic_g2p_particle(const MeshP& mp, int64_t p, co
     }
     if constexpr (ADV) {
         static_assert(!STAG && NC == 3, "advection needs the 3-component collocated velocity");
-#pragma unroll
-        for (int d = 0; d < 3; ++d)
-            x.set<double>(p, d, advect_coord(*adv, d, x.get<double>(p, d), (double)(PT)up[d]));
+        const double xo[3] = {x.get<double>(p, 0), x.get<double>(p, 1), x.get<double>(p, 2)};
+        const double uo[3] = {(double)(PT)up[0], (double)(PT)up[1], (double)(PT)up[2]};
+        advect_particle(*adv, p, xo, uo, [&](int d, double v) { x.set<double>(p, d, v); });
     }
 }
 

@@ -12,7 +12,7 @@
 #include <cmath>
 #include <mutex>
 
-#include "common.cuh"
+#include "binkey.cuh"
 
 namespace pb {
 
@@ -24,44 +24,6 @@ constexpr int kMaxDigitBits = 9;
 constexpr int kScanThreads = 1024;
 constexpr int kScanItems = 4;
 constexpr int kScanTile = kScanThreads * kScanItems;
-
-struct BinP {
-    MeshP mp;
-    int order;
-    int tile[3];
-    int nt[3];
-    int nb[3];
-    uint32_t tsize;
-    uint32_t nkeys;  // valid keys are < nkeys; out-of-mesh particles get nkeys
-};
-
-__device__ __forceinline__ uint32_t particle_key(const BinP& bp, const double xs[3])
-{
-    const int K = bp.order + 1;
-    const int first = (bp.order == 1) ? 0 : -1;
-    const double shift = (bp.order == 2) ? 0.5 : 0.0;
-    int b[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        const double x0 = logical_coord(xs[d], bp.mp.lo[d], bp.mp.rdx[d], shift);
-        const int s = (int)floor(x0) + first;
-        if (bp.mp.periodic[d]) {
-            int r = (s - bp.mp.own_lo[d]) % bp.nb[d];
-            if (r < 0) r += bp.nb[d];
-            b[d] = r;
-        } else {
-            if (s < 0 || s > bp.mp.ext[d] - K) return bp.nkeys;
-            b[d] = s;
-        }
-    }
-    const uint32_t tl = ((uint32_t)(b[0] / bp.tile[0]) * bp.nt[1] + (uint32_t)(b[1] / bp.tile[1])) *
-                            bp.nt[2] +
-                        (uint32_t)(b[2] / bp.tile[2]);
-    const uint32_t ll = ((uint32_t)(b[0] % bp.tile[0]) * bp.tile[1] + (uint32_t)(b[1] % bp.tile[1])) *
-                            bp.tile[2] +
-                        (uint32_t)(b[2] % bp.tile[2]);
-    return tl * bp.tsize + ll;
-}
 
 __global__ void key_kernel(BinP bp, int64_t n, PField x, uint32_t* __restrict__ keys,
                            uint32_t* __restrict__ vals)
@@ -76,7 +38,7 @@ __global__ void key_kernel(BinP bp, int64_t n, PField x, uint32_t* __restrict__ 
 
 __global__ void __launch_bounds__(kSortThreads)
 radix_hist_kernel(const uint32_t* __restrict__ keys, int64_t n, int shift, int bits,
-                  uint32_t* __restrict__ hist, int64_t nblk)
+                  uint32_t* __restrict__ hist, int64_t nblk, uint32_t kmax)
 {
     __shared__ uint32_t cnt[1 << kMaxDigitBits];
     const int nd = 1 << bits;
@@ -89,7 +51,7 @@ radix_hist_kernel(const uint32_t* __restrict__ keys, int64_t n, int shift, int b
     for (int r = 0; r < kSortItems; ++r) {
         const int64_t e = base + (int64_t)r * kSortThreads + threadIdx.x;
         const bool valid = e < n;
-        const uint32_t dig = valid ? (__ldg(keys + e) >> shift) & mask : 0xFFFFFFFFu;
+        const uint32_t dig = valid ? (min(__ldg(keys + e), kmax) >> shift) & mask : 0xFFFFFFFFu;
         const unsigned peers = __match_any_sync(0xFFFFFFFFu, dig);
         if (valid && lane == __ffs(peers) - 1) atomicAdd(&cnt[dig], (uint32_t)__popc(peers));
     }
@@ -100,7 +62,8 @@ radix_hist_kernel(const uint32_t* __restrict__ keys, int64_t n, int shift, int b
 __global__ void __launch_bounds__(kSortThreads)
 radix_scatter_kernel(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
                      uint32_t* __restrict__ kout, uint32_t* __restrict__ vout, int64_t n,
-                     int shift, int bits, const uint32_t* __restrict__ offs, int64_t nblk)
+                     int shift, int bits, const uint32_t* __restrict__ offs, int64_t nblk,
+                     uint32_t kmax)
 {
     __shared__ uint32_t wcnt[kSortWarps][1 << kMaxDigitBits];
     const int nd = 1 << bits;
@@ -116,8 +79,8 @@ radix_scatter_kernel(const uint32_t* __restrict__ kin, const uint32_t* __restric
     for (int r = 0; r < kSortItems; ++r) {
         const int64_t e = base + r * 32 + lane;
         const bool valid = e < n;
-        key[r] = valid ? __ldg(kin + e) : 0u;
-        val[r] = valid ? __ldg(vin + e) : 0u;
+        key[r] = valid ? min(__ldg(kin + e), kmax) : 0u;
+        val[r] = valid ? (vin ? __ldg(vin + e) : (uint32_t)e) : 0u;  // no vin: the index
         const uint32_t dig = valid ? (key[r] >> shift) & mask : 0xFFFFFFFFu;
         const unsigned peers = __match_any_sync(0xFFFFFFFFu, dig);
         uint32_t cur = 0;
@@ -309,27 +272,40 @@ struct SortPlan {
 
 static int64_t align256(int64_t v) { return (v + 255) & ~int64_t(255); }
 
-static picasso_status make_plan(const picasso_spline* sd, int64_t n, const int32_t tile[3],
-                                SortPlan* pl)
+picasso_status make_binp(const picasso_spline* sd, const int32_t tile[3], BinP* bp,
+                         int64_t* ntiles)
 {
-    picasso_status st = make_mesh(sd, &pl->bp.mp);
+    picasso_status st = make_mesh(sd, &bp->mp);
     if (st) return st;
-    if (!tile || n < 0 || n > 0xFFFFFFFELL) return PICASSO_ERR_INVALID_ARGUMENT;
-    pl->bp.order = sd->order;
+    if (!tile) return PICASSO_ERR_INVALID_ARGUMENT;
+    bp->order = sd->order;
     int64_t nt_total = 1, tsize = 1;
     for (int d = 0; d < 3; ++d) {
         if (tile[d] < 1) return PICASSO_ERR_INVALID_ARGUMENT;
-        pl->bp.tile[d] = tile[d];
-        pl->bp.nb[d] = sd->mesh.periodic[d] ? sd->mesh.own_extent[d] : sd->mesh.extent[d];
-        pl->bp.nt[d] = (pl->bp.nb[d] + tile[d] - 1) / tile[d];
-        nt_total *= pl->bp.nt[d];
+        bp->tile[d] = tile[d];
+        bp->tshift[d] = -1;
+        for (int sh = 0; sh < 31; ++sh)
+            if ((1 << sh) == tile[d]) bp->tshift[d] = sh;
+        bp->nb[d] = sd->mesh.periodic[d] ? sd->mesh.own_extent[d] : sd->mesh.extent[d];
+        bp->nt[d] = (bp->nb[d] + tile[d] - 1) / tile[d];
+        nt_total *= bp->nt[d];
         tsize *= tile[d];
     }
     const int64_t nkeys = nt_total * tsize;
     if (nkeys >= 0xFFFFFFFFLL) return PICASSO_ERR_OUT_OF_RANGE;
-    pl->bp.tsize = (uint32_t)tsize;
-    pl->bp.nkeys = (uint32_t)nkeys;
-    pl->ntiles = nt_total;
+    bp->tsize = (uint32_t)tsize;
+    bp->nkeys = (uint32_t)nkeys;
+    *ntiles = nt_total;
+    return PICASSO_OK;
+}
+
+static picasso_status make_plan(const picasso_spline* sd, int64_t n, const int32_t tile[3],
+                                SortPlan* pl)
+{
+    if (!sd || !tile || n < 0 || n > 0xFFFFFFFELL) return PICASSO_ERR_INVALID_ARGUMENT;
+    picasso_status st = make_binp(sd, tile, &pl->bp, &pl->ntiles);
+    if (st) return st;
+    const int64_t nkeys = pl->bp.nkeys;
     int bits = 1;
     while ((int64_t(1) << bits) <= nkeys) ++bits;  // keys are in [0, nkeys]
     pl->bits = bits;
@@ -372,22 +348,28 @@ extern "C" picasso_status picasso_cell_sort_workspace(const picasso_spline* sd,
     return PICASSO_OK;
 }
 
-extern "C" picasso_status picasso_cell_sort(const picasso_spline* sd, int64_t num_particles,
-                                            picasso_particle_field x_p, const int32_t tile[3],
-                                            int32_t chunk, uint32_t* key, uint32_t* perm,
-                                            int64_t* tile_offset, uint32_t* tile_items,
-                                            void* workspace, int64_t workspace_bytes,
-                                            picasso_bins* bins_out, const picasso_exec* exec)
+// The sort proper.  key_src == nullptr: keys from the positions x_p;
+// otherwise the first radix pass reads the caller's keys (clamped to nkeys)
+// and takes the particle index as its value.
+static picasso_status cell_sort_impl(const picasso_spline* sd, int64_t num_particles,
+                                     const picasso_particle_field* x_p, const uint32_t* key_src,
+                                     const int32_t tile[3], int32_t chunk, uint32_t* key,
+                                     uint32_t* perm, int64_t* tile_offset, uint32_t* tile_items,
+                                     void* workspace, int64_t workspace_bytes,
+                                     picasso_bins* bins_out, const picasso_exec* exec)
 {
     SortPlan pl;
     picasso_status st = make_plan(sd, num_particles, tile, &pl);
     if (st) return st;
-    if ((st = validate_pfield(num_particles, x_p, PICASSO_F64))) return st;
+    if (x_p && (st = validate_pfield(num_particles, *x_p, PICASSO_F64))) return st;
     if ((num_particles > 0 && (!key || !perm)) || !tile_offset || !tile_items || !workspace ||
         workspace_bytes < pl.bytes || chunk < 32)
         return PICASSO_ERR_INVALID_ARGUMENT;
+    if (!x_p && num_particles > 0 && (!key_src || key_src == key || key_src == perm))
+        return PICASSO_ERR_INVALID_ARGUMENT;
     if (reinterpret_cast<uintptr_t>(workspace) % 256) return PICASSO_ERR_INVALID_ARGUMENT;
     const int64_t n = num_particles;
+    const uint32_t kmax = pl.bp.nkeys;
     cudaStream_t s = stream_of(exec);
     char* ws = static_cast<char*>(workspace);
     uint32_t* wk = reinterpret_cast<uint32_t*>(ws + pl.off_keys);
@@ -404,25 +386,34 @@ extern "C" picasso_status picasso_cell_sort(const picasso_spline* sd, int64_t nu
         vb = wv;
     }
     if (n > 0) {
-        key_kernel<<<grid_for(n, 256), 256, 0, s>>>(pl.bp, n, make_pfield(x_p), ka, va);
+        const uint32_t* kin = ka;
+        const uint32_t* vin = va;
+        if (x_p) {
+            key_kernel<<<grid_for(n, 256), 256, 0, s>>>(pl.bp, n, make_pfield(*x_p), ka, va);
+        } else {
+            kin = key_src;
+            vin = nullptr;
+        }
         for (int pass = 0; pass < pl.passes; ++pass) {
             const int shift = pass * pl.width;
             const int bits = (shift + pl.width <= pl.bits) ? pl.width : pl.bits - shift;
-            radix_hist_kernel<<<(unsigned)pl.nblk, kSortThreads, 0, s>>>(ka, n, shift, bits, hist,
-                                                                          pl.nblk);
+            radix_hist_kernel<<<(unsigned)pl.nblk, kSortThreads, 0, s>>>(kin, n, shift, bits, hist,
+                                                                          pl.nblk, kmax);
             const int64_t m = (int64_t(1) << bits) * pl.nblk;
             const int64_t sb = (m + kScanTile - 1) / kScanTile;
             scan_reduce_kernel<<<(unsigned)sb, kScanThreads, 0, s>>>(hist, m, sums);
             scan_sums_kernel<<<1, kScanThreads, 0, s>>>(sums, sb);
             scan_apply_kernel<<<(unsigned)sb, kScanThreads, 0, s>>>(hist, scan, m, sums);
             radix_scatter_kernel<<<(unsigned)pl.nblk, kSortThreads, 0, s>>>(
-                ka, va, kb, vb, n, shift, bits, scan, pl.nblk);
+                kin, vin, kb, vb, n, shift, bits, scan, pl.nblk, kmax);
             uint32_t* t = ka;
             ka = kb;
             kb = t;
             t = va;
             va = vb;
             vb = t;
+            kin = ka;
+            vin = va;
         }
     }
     tile_offset_kernel<<<grid_for(pl.ntiles + 1, 256), 256, 0, s>>>(key, n, pl.ntiles, pl.bp.tsize,
@@ -451,6 +442,29 @@ extern "C" picasso_status picasso_cell_sort(const picasso_spline* sd, int64_t nu
         bins_out->tile_items = tile_items;
     }
     return PICASSO_OK;
+}
+
+extern "C" picasso_status picasso_cell_sort(const picasso_spline* sd, int64_t num_particles,
+                                            picasso_particle_field x_p, const int32_t tile[3],
+                                            int32_t chunk, uint32_t* key, uint32_t* perm,
+                                            int64_t* tile_offset, uint32_t* tile_items,
+                                            void* workspace, int64_t workspace_bytes,
+                                            picasso_bins* bins_out, const picasso_exec* exec)
+{
+    return cell_sort_impl(sd, num_particles, &x_p, nullptr, tile, chunk, key, perm, tile_offset,
+                          tile_items, workspace, workspace_bytes, bins_out, exec);
+}
+
+extern "C" picasso_status picasso_cell_sort_keys(const picasso_spline* sd, int64_t num_particles,
+                                                 const uint32_t* key_in, const int32_t tile[3],
+                                                 int32_t chunk, uint32_t* key, uint32_t* perm,
+                                                 int64_t* tile_offset, uint32_t* tile_items,
+                                                 void* workspace, int64_t workspace_bytes,
+                                                 picasso_bins* bins_out,
+                                                 const picasso_exec* exec)
+{
+    return cell_sort_impl(sd, num_particles, nullptr, key_in, tile, chunk, key, perm, tile_offset,
+                          tile_items, workspace, workspace_bytes, bins_out, exec);
 }
 
 extern "C" picasso_status picasso_permute(int64_t num_particles, int32_t ncomp,

@@ -804,9 +804,8 @@ __device__ void g2p_item(const G2PArgs& A, int64_t t, int64_t a, int64_t b, floa
         out[1] = make_float4(B[1][0], B[2][0], B[0][1], B[1][1]);
         out[2] = make_float4(B[2][1], B[0][2], B[1][2], B[2][2]);
         if constexpr (ADV) {
-#pragma unroll
-            for (int d = 0; d < 3; ++d)
-                A.x_out[3 * p + d] = advect_coord(A.adv, d, xp[d], (double)up[d]);
+            const double uo[3] = {(double)up[0], (double)up[1], (double)up[2]};
+            advect_particle(A.adv, p, xp, uo, [&](int d, double v) { A.x_out[3 * p + d] = v; });
         }
     }
 }

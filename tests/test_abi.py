@@ -172,6 +172,34 @@ def test_sort_workspace_and_key_range():
         _abi.ERR_OUT_OF_RANGE
 
 
+def test_sort_keys_and_key_emission_reject_on_host():
+    lib = _abi.load_library()
+    sp = _spline(n=16)
+    tile = (C.c_int32 * 3)(4, 4, 4)
+    nbytes = C.c_int64()
+    assert lib.picasso_cell_sort_workspace(C.byref(sp), 100, tile, C.byref(nbytes)) == 0
+    ws, nb = 1 << 12, nbytes.value
+
+    def sort_keys(key_in, key, n=100):
+        return lib.picasso_cell_sort_keys(C.byref(sp), n, key_in, tile, 256, key, 1 << 20,
+                                          1 << 21, 1 << 22, ws, nb, None, None)
+    assert sort_keys(1 << 16, 1 << 16) == _abi.ERR_INVALID_ARGUMENT  # key_in is the output
+    assert sort_keys(None, 1 << 16) == _abi.ERR_INVALID_ARGUMENT
+    assert lib.picasso_cell_sort_keys(C.byref(sp), 100, 1 << 16, tile, 256, 1 << 17, 1 << 20,
+                                      1 << 21, 1 << 22, ws, nb - 1, None, None) == \
+        _abi.ERR_INVALID_ARGUMENT  # workspace too small
+    x, c, u = _pf(), _pf(), _gf()
+    c.tile_stride = 12
+    bad = (C.c_int32 * 3)(0, 4, 4)
+    assert lib.picasso_apic_g2p_advect_keys(C.byref(sp), 10, x, u, c, 0.1, None, 1 << 16,
+                                            None) == _abi.ERR_INVALID_ARGUMENT
+    assert lib.picasso_apic_g2p_advect_keys(C.byref(sp), 10, x, u, c, 0.1, bad, 1 << 16,
+                                            None) == _abi.ERR_INVALID_ARGUMENT
+    assert lib.picasso_apic_g2p_advect_keys(C.byref(sp), 10, x, u, c, 0.1, tile, None,
+                                            None) == _abi.ERR_INVALID_ARGUMENT
+    assert lib.picasso_apic_g2p_advect_keys(C.byref(sp), 0, x, u, c, 0.1, tile, None, None) == 0
+
+
 def _batch_instance(f32=True):
     inst = _abi.BatchInstance()
     inst.spline = _spline()

@@ -44,6 +44,9 @@ int main(int argc, char**) {
         APIC::p2g(m, c, u, u, sd);
         APIC::g2p(u, c, sd);
         APIC::g2pAdvect(u, c, sd, 0.1);
+        const int32_t tile[3] = {4, 8, 8};
+        uint32_t* keys = nullptr;
+        APIC::g2pAdvect(u, c, sd, 0.1, tile, keys);
         PolyPIC::g2p(u, c, sd);
         picasso_grid_update_params prm{};
         B200::gridUpdate(mesh, u, u, u, prm, u);
