@@ -17,6 +17,7 @@
 #pragma once
 
 #include <cstdint>
+#include <map>
 #include <stdexcept>
 #include <string>
 
@@ -44,7 +45,36 @@ struct Edge {
     static_assert(D >= 0 && D < 3, "Edge dimension out of bounds");
     static constexpr int value = PICASSO_EDGE_I + D;
 };
+// the particle loop of GridOperator::apply
+struct Particle {};
 }  // namespace FieldLocation
+
+// Field value types: a field tag derives from one of these and gives a
+// static label() (the tags of the reference's tests, tstAPIC.hpp:35-48).
+namespace Field {
+template <class T>
+struct Scalar {
+    using value_type = T;
+    static constexpr int rows = 1, cols = 1, size = 1;
+};
+template <class T, int N>
+struct Vector {
+    using value_type = T;
+    static constexpr int rows = 1, cols = N, size = N;
+};
+template <class T, int R, int C>
+struct Matrix {
+    using value_type = T;
+    static constexpr int rows = R, cols = C, size = R * C;
+};
+}  // namespace Field
+
+// A field at a mesh location (FieldLayout<Location, Tag>).
+template <class Location, class Tag>
+struct FieldLayout {
+    using location = Location;
+    using tag = Tag;
+};
 
 template <int N>
 struct InterpolationOrder {
@@ -343,6 +373,235 @@ class Batch {
 
   private:
     picasso_batch* b_ = nullptr;
+};
+
+// ---------------------------------------------------------------------------
+// GridOperator-style bulk calls (src/Picasso_GridOperator.hpp:380-642,
+// src/Picasso_FieldManager.hpp:66-140)
+// ---------------------------------------------------------------------------
+// In Picasso an application registers grid fields in a FieldManager, keeps
+// particles in a Cabana ParticleList and calls
+//   op.apply("p2g", FieldLocation::Particle(), exec, fm, pl, functor)
+// with a device functor that calls APIC::p2g per particle.  Here the functor
+// is one of the transfer descriptors below (it names the fields the transfer
+// reads and writes), and apply() runs the transfer as one call over the
+// particle list.  As in GridOperator::applyImpl, the scatter fields of a
+// particle transfer start from zero.  Halo exchange between ranks is the
+// caller's (picasso_b200.dist in Python); periodic meshes wrap on one rank.
+
+// Grid fields in device memory, keyed by (location, tag label); the arrays
+// are borrowed.  Each location carries the picasso_mesh its arrays index
+// (extent with ghosts, owned range, low corner, cell size).
+class FieldManager {
+  public:
+    template <class Location>
+    void setMesh(Location, const picasso_mesh& mesh)
+    {
+        const int loc = Location::value;  // (no odr-use of the constant in C++14)
+        meshes_[loc] = mesh;
+    }
+    template <class Location>
+    const picasso_mesh& mesh(Location) const
+    {
+        const int loc = Location::value;
+        auto it = meshes_.find(loc);
+        if (it == meshes_.end())
+            throw Error(PICASSO_ERR_INVALID_ARGUMENT, "FieldManager: no mesh for location");
+        return it->second;
+    }
+    template <class Location, class Tag>
+    void add(Location, Tag, const GridArray& array)
+    {
+        if (array.components != Tag::size)
+            throw Error(PICASSO_ERR_INVALID_ARGUMENT,
+                        "FieldManager::add: " + Tag::label() + " component count");
+        fields_[key(Location::value, Tag::label())] = array;
+    }
+    template <class Layout>
+    void add(Layout, const GridArray& array)
+    {
+        add(typename Layout::location(), typename Layout::tag(), array);
+    }
+    template <class Location, class Tag>
+    const GridArray& array(Location, Tag) const
+    {
+        auto it = fields_.find(key(Location::value, Tag::label()));
+        if (it == fields_.end())
+            throw Error(PICASSO_ERR_INVALID_ARGUMENT, "FieldManager: no field " + Tag::label());
+        return it->second;
+    }
+    template <class Layout>
+    const GridArray& array(Layout) const
+    {
+        return array(typename Layout::location(), typename Layout::tag());
+    }
+
+  private:
+    static std::string key(int location, const std::string& label)
+    {
+        return std::to_string(location) + "/" + label;
+    }
+    std::map<int, picasso_mesh> meshes_;
+    std::map<std::string, GridArray> fields_;
+};
+
+// Particle members in device memory, keyed by tag label (borrowed), and the
+// optional sorted bins of the current particle order (picasso_cell_sort
+// followed by picasso_permute of every member).
+class ParticleList {
+  public:
+    explicit ParticleList(int64_t n) : n_(n) {}
+    int64_t size() const { return n_; }
+    template <class Tag>
+    void add(Tag, const ParticleMember& member)
+    {
+        if (member.n != n_ || member.components != Tag::size)
+            throw Error(PICASSO_ERR_INVALID_ARGUMENT, "ParticleList::add: " + Tag::label());
+        members_[Tag::label()] = member;
+    }
+    template <class Tag>
+    const ParticleMember& get(Tag) const
+    {
+        auto it = members_.find(Tag::label());
+        if (it == members_.end())
+            throw Error(PICASSO_ERR_INVALID_ARGUMENT, "ParticleList: no member " + Tag::label());
+        return it->second;
+    }
+    void setBins(const picasso_bins* bins) { bins_ = bins; }
+    const picasso_bins* bins() const { return bins_; }
+
+  private:
+    int64_t n_;
+    std::map<std::string, ParticleMember> members_;
+    const picasso_bins* bins_ = nullptr;
+};
+
+// Transfer descriptors for GridOperator::apply over FieldLocation::Particle.
+// Particle tags: Position (3 x FP64), Mass, Affine (4 x 3 APIC c_p) or
+// Velocity / Modes (PolyPIC u_p, c_p); grid tags at `Location`.
+template <class Location, class Order, class Position, class Mass, class Affine, class GridMass,
+          class GridMomentum>
+struct APICP2G {};
+template <class Location, class Order, class Position, class Affine, class GridVelocity>
+struct APICG2P {};
+// G2P followed by x_p += dt u_p (collocated, 3 components)
+template <class Location, class Order, class Position, class Affine, class GridVelocity>
+struct APICG2PAdvect {
+    double dt;
+};
+template <class Location, class Order, class Position, class Mass, class Velocity, class Modes,
+          class GridMomentum, class GridMass>
+struct PolyPICP2G {
+    double dt;
+};
+template <class Location, class Order, class Position, class Modes, class GridVelocity>
+struct PolyPICG2P {};
+
+// Grid descriptors for GridOperator::apply over a mesh location.
+template <class GridMass, class GridMomentum, class GridVelocity>
+struct VelocityUpdate {  // u = mu / m where m > mass_threshold, else 0
+    double mass_threshold;
+};
+template <class GridMass, class GridMomentum, class GridVelocity>
+struct MomentumUpdate {  // picasso_grid_update without a force field
+    picasso_grid_update_params params;
+};
+
+template <class FieldDependencies = void>
+class GridOperator {
+  public:
+    // Fields are registered by the application (they are borrowed), so there
+    // is nothing to add; kept for the call sequence of Picasso.
+    void setup(FieldManager&) {}
+
+    template <class Op>
+    void apply(const std::string& label, FieldLocation::Particle, const Exec& exec,
+               const FieldManager& fm, const ParticleList& pl, const Op& op) const
+    {
+        Exec ex = exec;
+        if (!ex.exec.bins) ex.exec.bins = pl.bins();
+        run(label, ex, fm, pl, op);
+    }
+
+    template <class Location, class Op>
+    void apply(const std::string& label, Location loc, const Exec& exec, const FieldManager& fm,
+               const Op& op) const
+    {
+        run_grid(label, loc, exec, fm, op);
+    }
+
+  private:
+    template <class L, class O, class P, class M, class A, class GM, class GU>
+    static void run(const std::string&, const Exec& ex, const FieldManager& fm,
+                    const ParticleList& pl, const APICP2G<L, O, P, M, A, GM, GU>&)
+    {
+        const picasso_mesh& mesh = fm.mesh(L());
+        const GridArray& m_i = fm.array(L(), GM());
+        const GridArray& mu_i = fm.array(L(), GU());
+        zero(mesh, m_i, ex);
+        zero(mesh, mu_i, ex);
+        auto sd = createSpline(L(), O(), mesh, pl.get(P()));
+        APIC::p2g(pl.get(M()), pl.get(A()), m_i, mu_i, sd, ex);
+    }
+    template <class L, class O, class P, class A, class GV>
+    static void run(const std::string&, const Exec& ex, const FieldManager& fm,
+                    const ParticleList& pl, const APICG2P<L, O, P, A, GV>&)
+    {
+        auto sd = createSpline(L(), O(), fm.mesh(L()), pl.get(P()));
+        APIC::g2p(fm.array(L(), GV()), pl.get(A()), sd, ex);
+    }
+    template <class L, class O, class P, class A, class GV>
+    static void run(const std::string&, const Exec& ex, const FieldManager& fm,
+                    const ParticleList& pl, const APICG2PAdvect<L, O, P, A, GV>& op)
+    {
+        auto sd = createSpline(L(), O(), fm.mesh(L()), pl.get(P()));
+        APIC::g2pAdvect(fm.array(L(), GV()), pl.get(A()), sd, op.dt, ex);
+    }
+    template <class L, class O, class P, class M, class V, class C, class GU, class GM>
+    static void run(const std::string&, const Exec& ex, const FieldManager& fm,
+                    const ParticleList& pl, const PolyPICP2G<L, O, P, M, V, C, GU, GM>& op)
+    {
+        const picasso_mesh& mesh = fm.mesh(L());
+        const GridArray& mu_i = fm.array(L(), GU());
+        const GridArray& m_i = fm.array(L(), GM());
+        zero(mesh, mu_i, ex);
+        zero(mesh, m_i, ex);
+        auto sd = createSpline(L(), O(), mesh, pl.get(P()));
+        PolyPIC::p2g(pl.get(M()), pl.get(V()), pl.get(C()), mu_i, m_i, op.dt, sd, ex);
+    }
+    template <class L, class O, class P, class C, class GV>
+    static void run(const std::string&, const Exec& ex, const FieldManager& fm,
+                    const ParticleList& pl, const PolyPICG2P<L, O, P, C, GV>&)
+    {
+        auto sd = createSpline(L(), O(), fm.mesh(L()), pl.get(P()));
+        PolyPIC::g2p(fm.array(L(), GV()), pl.get(C()), sd, ex);
+    }
+
+    template <class L, class GM, class GU, class GV>
+    static void run_grid(const std::string&, L, const Exec& ex, const FieldManager& fm,
+                         const VelocityUpdate<GM, GU, GV>& op)
+    {
+        const GridArray& mu_i = fm.array(L(), GU());
+        picasso_grid_field none{};
+        check(picasso_grid_velocity(&fm.mesh(L()), mu_i.components, fm.array(L(), GM()).field,
+                                    mu_i.field, op.mass_threshold, fm.array(L(), GV()).field,
+                                    none, &ex.exec),
+              "GridOperator::apply(VelocityUpdate)");
+    }
+    template <class L, class GM, class GU, class GV>
+    static void run_grid(const std::string&, L, const Exec& ex, const FieldManager& fm,
+                         const MomentumUpdate<GM, GU, GV>& op)
+    {
+        gridUpdate(fm.mesh(L()), fm.array(L(), GM()), fm.array(L(), GU()), GridArray{},
+                   op.params, fm.array(L(), GV()), ex);
+    }
+
+    // scatter fields start from zero (GridOperator.hpp:532-533)
+    static void zero(const picasso_mesh& mesh, const GridArray& a, const Exec& ex)
+    {
+        check(picasso_grid_fill(&mesh, a.components, a.field, 0.0, &ex.exec),
+              "GridOperator::apply (zero scatter field)");
+    }
 };
 
 }  // namespace B200

@@ -31,6 +31,11 @@ def test_header_wrappers_instantiate(tmp_path):
     src.write_text(r'''
 #include "picasso_b200.hpp"
 using namespace Picasso;
+struct PX : Field::Vector<double, 3> { static std::string label() { return "x"; } };
+struct PM : Field::Scalar<double> { static std::string label() { return "m"; } };
+struct PC : Field::Matrix<double, 4, 3> { static std::string label() { return "c"; } };
+struct GM : Field::Scalar<double> { static std::string label() { return "gm"; } };
+struct GV : Field::Vector<double, 3> { static std::string label() { return "gv"; } };
 int main(int argc, char**) {
     if (argc > 100) {  // never taken: only instantiation and linking are tested
         picasso_mesh mesh{};
@@ -52,6 +57,27 @@ int main(int argc, char**) {
         B200::gridUpdate(mesh, u, u, u, prm, u);
         B200::Batch batch(nullptr, 0);
         batch.step();
+        B200::FieldManager fm;
+        fm.setMesh(FieldLocation::Node(), mesh);
+        fm.add(FieldLocation::Node(), GV(), u);
+        B200::ParticleList pl(1);
+        pl.add(PX(), x);
+        B200::GridOperator<> op;
+        op.setup(fm);
+        using N = FieldLocation::Node;
+        using Q = InterpolationOrder<2>;
+        op.apply("p2g", FieldLocation::Particle(), B200::Exec(), fm, pl,
+                 B200::APICP2G<N, Q, PX, PM, PC, GM, GV>());
+        op.apply("g2p", FieldLocation::Particle(), B200::Exec(), fm, pl,
+                 B200::APICG2P<N, Q, PX, PC, GV>());
+        op.apply("g2px", FieldLocation::Particle(), B200::Exec(), fm, pl,
+                 B200::APICG2PAdvect<N, Q, PX, PC, GV>{0.1});
+        op.apply("pp2g", FieldLocation::Particle(), B200::Exec(), fm, pl,
+                 B200::PolyPICP2G<N, InterpolationOrder<1>, PX, PM, PC, PC, GV, GM>{0.1});
+        op.apply("pg2p", FieldLocation::Particle(), B200::Exec(), fm, pl,
+                 B200::PolyPICG2P<N, InterpolationOrder<1>, PX, PC, GV>());
+        op.apply("vel", N(), B200::Exec(), fm, B200::VelocityUpdate<GM, GV, GV>{1e-12});
+        op.apply("upd", N(), B200::Exec(), fm, B200::MomentumUpdate<GM, GV, GV>{prm});
     }
     return 0;
 }
@@ -62,14 +88,33 @@ int main(int argc, char**) {
                     str(tmp_path / "inst")], check=True)
 
 
-@pytest.mark.gpu
-def test_shim_reproduces_golden(cuda, tmp_path):
-    exe = str(tmp_path / "shim_golden")
+def _run_golden_program(src, tmp_path):
+    exe = str(tmp_path / os.path.splitext(os.path.basename(src))[0])
     lib = os.path.join(ROOT, "picasso_b200")
-    subprocess.run([CXX, "-std=c++17", "-O2", "-I", INC, "-I", CUDA + "/include", SRC, "-o", exe,
+    subprocess.run([CXX, "-std=c++17", "-O2", "-I", INC, "-I", CUDA + "/include", src, "-o", exe,
                     "-L", lib, "-lpicasso_b200", "-L", CUDA + "/lib64", "-lcudart",
                     "-Wl,-rpath," + lib + ":" + CUDA + "/lib64"], check=True)
     out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split("\n")
+    _check_golden_output(out)
+    return out
+
+
+@pytest.mark.gpu
+def test_shim_reproduces_golden(cuda, tmp_path):
+    _run_golden_program(SRC, tmp_path)
+
+
+@pytest.mark.gpu
+def test_grid_operator_reproduces_golden(cuda, tmp_path):
+    """GridOperator::apply with FieldManager / ParticleList and the transfer
+    descriptors; the scatter fields start as garbage and apply() zeroes them."""
+    out = _run_golden_program(os.path.join(ROOT, "tests", "cpp", "grid_operator_golden.cpp"),
+                              tmp_path)
+    outside = [float(l.split()[1]) for l in out if l.startswith("outside ")]
+    assert outside == [0.0]
+
+
+def _check_golden_output(out):
     c = np.array([float(l.split()[2]) for l in out if l.startswith("c ")])
     nodes = np.array([[float(v) for v in l.split()[2:]] for l in out if l.startswith("node ")])
     ck = golden()["apic"]["checks"]["2"]
