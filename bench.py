@@ -68,6 +68,8 @@ def parse():
     ap.add_argument("--adv-steps", type=int, default=10)
     ap.add_argument("--adv-tile", type=int, nargs=3, default=[4, 4, 8])
     ap.add_argument("--pp-grid", type=int, default=128)
+    ap.add_argument("--pp-tile", type=int, nargs=3, default=[4, 8, 8])
+    ap.add_argument("--pp-chunk", type=int, default=1024)
     ap.add_argument("--batch-instances", type=int, default=512)
     ap.add_argument("--batch-seed", type=int, default=4)
     ap.add_argument("--batch-forms", default="fp32,fp64")
@@ -586,10 +588,11 @@ def run_polypic(args, peak):
     n = x.shape[0]
     m64, _ = workloads.particle_state(n, seed)
     res = {"workload": "PolyPIC, %d^3 periodic, 8 ppc uniform, cell-sorted, per step: fill, "
-                       "P2G, velocity, G2P" % g, "particles": n}
+                       "P2G, velocity, G2P (FP32 form: tiled kernels, tile %s, work items of %d)"
+                       % (g, list(args.pp_tile), args.pp_chunk), "particles": n}
     for order, nm in ((2, 27), (1, 8)):
         sd0 = pb.create_spline(loc, order, mesh, x)
-        _, perm, _ = pb.cell_sort(sd0, (4, 8, 8))
+        _, perm, bins = pb.cell_sort(sd0, tuple(args.pp_tile), chunk=args.pp_chunk)
         modes = workloads.polypic_modes(n, nm, seed)
         xs, ms, us = pb.permute_members(perm, x, m64, modes)
         sd = pb.create_spline(loc, order, mesh, xs)
@@ -615,13 +618,14 @@ def run_polypic(args, peak):
                 if ev is not None:
                     ev[0].record()
                 pb.grid_fill(desc, fill, 0.0, ncomp=4)
-                pb.PolyPIC.p2g(mm, c, c, gmu, gm, 0.1 / g, sd)
+                # the FP32 form takes the tiled kernels (bins); FP64 the plain ones
+                pb.PolyPIC.p2g(mm, c, c, gmu, gm, 0.1 / g, sd, bins=bins if f32 else None)
                 if ev is not None:
                     ev[1].record()
                 pb.grid_velocity(desc, gm, gmu, u, 1e-12)
                 if ev is not None:
                     ev[2].record()
-                pb.PolyPIC.g2p(u, c, sd)
+                pb.PolyPIC.g2p(u, c, sd, bins=bins if f32 else None)
                 if ev is not None:
                     ev[3].record()
 

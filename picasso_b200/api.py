@@ -348,12 +348,14 @@ class PolyPIC:
     """Picasso::PolyPIC transfers (linear 8 modes; quadratic 27 modes)."""
 
     @staticmethod
-    def p2g(m_p, u_p, c_p, mu_i, m_i, dt, sd, stream=None, error_count=None):
-        """PolyPIC::p2g(m_p, u_p, c_p, mu_i, m_i, dt, sd) -- field before mass."""
+    def p2g(m_p, u_p, c_p, mu_i, m_i, dt, sd, stream=None, error_count=None, bins=None):
+        """PolyPIC::p2g(m_p, u_p, c_p, mu_i, m_i, dt, sd) -- field before mass.
+        With bins (cell-sorted particles) the FP32 form runs the tiled kernel
+        (bit-identical grid)."""
         ncomp = c_p.shape[2]
         _check_grid_extent(m_i, sd.desc.mesh)
         _check_grid_extent(mu_i, sd.desc.mesh)
-        ex = _exec(stream, error_count, None)
+        ex = _exec(stream, error_count, bins)
         check(_lib().picasso_polypic_p2g(C.byref(sd.desc), sd.num_particles, ncomp,
                                          particle_field(sd.x), particle_field(m_p),
                                          particle_field(u_p), particle_field(c_p),
@@ -361,11 +363,12 @@ class PolyPIC:
                                          C.byref(ex.desc)), "PolyPIC::p2g")
 
     @staticmethod
-    def g2p(u_i, c_p, sd, stream=None, error_count=None):
-        """PolyPIC::g2p(u_i, c_p, sd)."""
+    def g2p(u_i, c_p, sd, stream=None, error_count=None, bins=None):
+        """PolyPIC::g2p(u_i, c_p, sd).  With bins the FP32 form runs the tiled
+        kernel (bit-identical c_p)."""
         ncomp = c_p.shape[2]
         _check_grid_extent(u_i, sd.desc.mesh)
-        ex = _exec(stream, error_count, None)
+        ex = _exec(stream, error_count, bins)
         check(_lib().picasso_polypic_g2p(C.byref(sd.desc), sd.num_particles, ncomp,
                                          particle_field(sd.x), grid_field(u_i),
                                          particle_field(c_p), C.byref(ex.desc)),

@@ -9,6 +9,7 @@
 //   c_r = sum_i w_i s_r(r_i) u_i / sum_i w_i s_r(r_i)^2
 // (for linear splines these reduce to w and dw/dx, PolyPIC.hpp:269-284).
 #include "common.cuh"
+#include "tiled.cuh"
 #include "transfer.cuh"
 
 namespace pb {
@@ -77,25 +78,42 @@ __device__ __forceinline__ void inverse3(const R a[9], R inv[9])
 // ---------------------------------------------------------------------------
 // P2G: PolyPIC.hpp:41-130 (collocated) and :140-229 (staggered)
 // ---------------------------------------------------------------------------
-template <int ORDER, int NC, bool STAG, class PT, class R, class ACC>
-__global__ void __launch_bounds__(128)
-polypic_p2g_kernel(MeshP mp, int64_t n, PField x, PField m, PField u, PField c, GField gmu,
-                   GField gm, R dt, int col, R scale_mu, R scale_m, int* err)
-{
-    constexpr int K = SplineTraits<ORDER>::K;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
-        Spline1D<ORDER, R> sp[3];
-        int idx[3][K];
+// Spline and stencil indices of a particle on the whole local mesh (periodic
+// wrap, bounds check): the placement of the plain kernels.
+template <int ORDER, class R>
+struct MeshPlace {
+    const MeshP& mp;
+    __device__ __forceinline__ bool operator()(const double xp[3], Spline1D<ORDER, R> sp[3],
+                                               int idx[3][SplineTraits<ORDER>::K]) const
+    {
         bool ok = true;
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-            eval_spline<ORDER>(x.get<double>(p, d), mp.lo[d], mp.dx[d], mp.rdx[d], sp[d]);
-            ok = ok && resolve_stencil<K>(mp, d, sp[d].s0, idx[d]);
+            eval_spline<ORDER>(xp[d], mp.lo[d], mp.dx[d], mp.rdx[d], sp[d]);
+            ok = ok && resolve_stencil<SplineTraits<ORDER>::K>(mp, d, sp[d].s0, idx[d]);
         }
-        if (!ok) {
+        return ok;
+    }
+};
+
+// One particle.  place(xp, sp, idx) evaluates the spline and the stencil's
+// grid indices (false: skip the particle); acc(f, i, j, k, v) adds v to grid
+// field f (0 mass, 1 + d momentum component d); mode(v) returns c_p value v
+// (element v of the particle's record).
+template <int ORDER, int NC, bool STAG, class PT, class R, class Place, class Acc, class Mode>
+__device__ __forceinline__ void polypic_p2g_particle(const MeshP& mp, int64_t p, const PField& x,
+                                                     const PField& m, const PField& u, R dt,
+                                                     int col, int* err, Place&& place, Acc&& acc,
+                                                     Mode&& mode)
+{
+    constexpr int K = SplineTraits<ORDER>::K;
+    {
+        Spline1D<ORDER, R> sp[3];
+        int idx[3][K];
+        const double xp[3] = {x.get<double>(p, 0), x.get<double>(p, 1), x.get<double>(p, 2)};
+        if (!place(xp, sp, idx)) {
             if (err) atomicAdd(err, 1);
-            continue;
+            return;
         }
         const R mass = (R)m.get<PT>(p, 0);
         // affine material motion operator and its inverse (PolyPIC.hpp:81-87)
@@ -136,8 +154,8 @@ polypic_p2g_kernel(MeshP mp, int64_t n, PField x, PField m, PField u, PField c, 
                     for (int cc = 0; cc < D; ++cc)
 #pragma unroll
                         for (int e = 0; e < CB; ++e)
-                            cp[a][b][cc][e] = (R)c.get<PT>(
-                                p, mode_of(a, b, cc) * ncp + (STAG ? col : d0 + e));
+                            cp[a][b][cc][e] =
+                                (R)mode(mode_of(a, b, cc) * ncp + (STAG ? col : d0 + e));
             // 27 FP64 modes: i-planes one after the other (not unrolled: bounds
             // the live range of the 9-node plane bodies, which would spill)
 #pragma unroll(sizeof(R) == 8 && ORDER == 2 ? 1 : K)
@@ -181,37 +199,92 @@ polypic_p2g_kernel(MeshP mp, int64_t n, PField x, PField m, PField u, PField c, 
                                 }
                                 sa += f[0][a] * sb;
                             }
-                            ACC::add(gmu, gi, idx[1][j], idx[2][k], d0 + e, wm * sa, scale_mu);
+                            acc(1 + d0 + e, gi, idx[1][j], idx[2][k], wm * sa);
                         }
-                        if (d0 == 0) ACC::add(gm, gi, idx[1][j], idx[2][k], 0, wm, scale_m);
+                        if (d0 == 0) acc(0, gi, idx[1][j], idx[2][k], wm);
                     }
             }
         }
     }
 }
 
+// Modes per particle record (c_p rows): 8 linear, 27 quadratic.
+template <int ORDER>
+struct PPModes {
+    static constexpr int value = ORDER == 1 ? 8 : 27;
+};
+
+// Shared-memory records of a warp's 32 consecutive particles (packed c_p of
+// NV values each, at an odd stride so that the 32 lanes' records start on
+// distinct banks): the record of every particle is read or written by the
+// warp with coalesced accesses instead of NV strided accesses per thread.
+template <class PT, int NV>
+struct WarpRecords {
+    static constexpr int NVP = NV | 1;
+    PT* buf;
+    static constexpr size_t kBytesPerWarp = sizeof(PT) * 32 * NVP;
+    __device__ __forceinline__ PT& at(int lane, int v) const { return buf[lane * NVP + v]; }
+    // records of particles p0 .. p0 + cnt - 1 from packed storage
+    __device__ __forceinline__ void load(const PT* src, int cnt, int lane) const
+    {
+        for (int e = lane; e < cnt * NV; e += 32) {
+            const int q = e / NV;
+            buf[q * NVP + (e - q * NV)] = __ldg(src + e);
+        }
+        __syncwarp();
+    }
+    // records of the particles in `mask` (bit q: particle p0 + q) to packed
+    // storage
+    __device__ __forceinline__ void store(PT* dst, int cnt, unsigned mask, int lane) const
+    {
+        __syncwarp();
+        for (int e = lane; e < cnt * NV; e += 32) {
+            const int q = e / NV;
+            if ((mask >> q) & 1u) dst[e] = buf[q * NVP + (e - q * NV)];
+        }
+        __syncwarp();
+    }
+};
+
+template <int ORDER, int NC, bool STAG, class PT, class R, class ACC>
+__global__ void __launch_bounds__(128)
+polypic_p2g_kernel(MeshP mp, int64_t n, PField x, PField m, PField u, PField c, GField gmu,
+                   GField gm, R dt, int col, R scale_mu, R scale_m, int* err)
+{
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const MeshPlace<ORDER, R> place{mp};
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride)
+        polypic_p2g_particle<ORDER, NC, STAG, PT, R>(
+            mp, p, x, m, u, dt, col, err, place,
+            [&](int f, int i, int j, int k, R v) {
+                if (f == 0) ACC::add(gm, i, j, k, 0, v, scale_m);
+                else ACC::add(gmu, i, j, k, f - 1, v, scale_mu);
+            },
+            [&](int v) { return c.get<PT>(p, v); });
+}
+
 // ---------------------------------------------------------------------------
 // G2P: PolyPIC.hpp:236-293 (collocated) and :300-358 (staggered)
 // ---------------------------------------------------------------------------
-template <int ORDER, int NC, bool STAG, class GT, class PT, class R>
-__global__ void __launch_bounds__(128)
-polypic_g2p_kernel(MeshP mp, int64_t n, PField x, GField u, PField c, int col, int* err)
+// One particle; emit(v, value) receives c_p value v (element v of the
+// particle's record).  False if the particle was skipped (stencil outside a
+// non-periodic mesh): then nothing is emitted.
+// place: as for polypic_p2g_particle; grid(i, j, k, c) returns component c
+// of u at stencil indices (i, j, k).
+template <int ORDER, int NC, bool STAG, class PT, class R, class Place, class Grid, class Emit>
+__device__ __forceinline__ bool polypic_g2p_particle(const MeshP& mp, int64_t p, const PField& x,
+                                                     int col, int* err, Place&& place,
+                                                     Grid&& grid, Emit&& emit)
 {
     constexpr int K = SplineTraits<ORDER>::K;
     constexpr int NCU = STAG ? 1 : NC;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
+    {
         Spline1D<ORDER, R> sp[3];
         int idx[3][K];
-        bool ok = true;
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            eval_spline<ORDER>(x.get<double>(p, d), mp.lo[d], mp.dx[d], mp.rdx[d], sp[d]);
-            ok = ok && resolve_stencil<K>(mp, d, sp[d].s0, idx[d]);
-        }
-        if (!ok) {
+        const double xp[3] = {x.get<double>(p, 0), x.get<double>(p, 1), x.get<double>(p, 2)};
+        if (!place(xp, sp, idx)) {
             if (err) atomicAdd(err, 1);
-            continue;
+            return false;
         }
         // per-dimension factors G[d][degree][knot]
         R G[3][3][K];
@@ -269,7 +342,7 @@ polypic_g2p_kernel(MeshP mp, int64_t n, PField x, GField u, PField c, int col, i
                     for (int k = 0; k < K; ++k)
 #pragma unroll
                         for (int e = 0; e < CB; ++e)
-                            ue[k][e] = (R)__ldg(u.ptr<GT>(idx[0][i], idx[1][j], idx[2][k], d0 + e));
+                            ue[k][e] = grid(idx[0][i], idx[1][j], idx[2][k], d0 + e);
 #pragma unroll
                     for (int cc = 0; cc < D; ++cc)
 #pragma unroll
@@ -299,47 +372,303 @@ polypic_g2p_kernel(MeshP mp, int64_t n, PField x, GField u, PField c, int col, i
                     for (int cc = 0; cc < D; ++cc)
 #pragma unroll
                         for (int e = 0; e < CB; ++e)
-                            c.set<PT>(p, mode_of(a, b, cc) * ncp + (STAG ? col : d0 + e),
-                                      (PT)cp[a][b][cc][e]);
+                            emit(mode_of(a, b, cc) * ncp + (STAG ? col : d0 + e),
+                                 (PT)cp[a][b][cc][e]);
         }
     }
+    return true;
+}
+
+// WS: c_p is packed and written through WarpRecords (see polypic_p2g_kernel).
+template <int ORDER, int NC, bool STAG, class GT, class PT, class R, bool WS>
+__global__ void __launch_bounds__(128)
+polypic_g2p_kernel(MeshP mp, int64_t n, PField x, GField u, PField c, int col, int* err)
+{
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const MeshPlace<ORDER, R> place{mp};
+    auto grid = [&](int i, int j, int k, int cc) { return (R)__ldg(u.ptr<GT>(i, j, k, cc)); };
+    if constexpr (!WS) {
+        for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride)
+            polypic_g2p_particle<ORDER, NC, STAG, PT, R>(
+                mp, p, x, col, err, place, grid, [&](int v, PT val) { c.set<PT>(p, v, val); });
+    } else {
+        constexpr int NV = PPModes<ORDER>::value * NC;
+        extern __shared__ __align__(16) unsigned char pp_smem[];
+        const int lane = threadIdx.x & 31;
+        const WarpRecords<PT, NV> rec{reinterpret_cast<PT*>(pp_smem) +
+                                      (threadIdx.x >> 5) * 32 * WarpRecords<PT, NV>::NVP};
+        PT* cbase = reinterpret_cast<PT*>(c.data);
+        for (int64_t p0 = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); p0 < n;
+             p0 += stride) {
+            const int cnt = (int)min((int64_t)32, n - p0);
+            bool wrote = false;
+            if (lane < cnt)
+                wrote = polypic_g2p_particle<ORDER, NC, STAG, PT, R>(
+                    mp, p0 + lane, x, col, err, place, grid,
+                    [&](int v, PT val) { rec.at(lane, v) = val; });
+            rec.store(cbase + p0 * NV, cnt, __ballot_sync(0xFFFFFFFFu, wrote), lane);
+        }
+    }
+}
+
+// c_p stored packed: the record of particle p (all modes and components) at
+// element p * NV, 16-byte aligned.
+template <int ORDER, int NC, class PT>
+static bool packed_record(const PField& c)
+{
+    constexpr int NV = PPModes<ORDER>::value * NC;
+    return c.shift == 0 && c.tile_stride == NV && c.comp_stride == 1 &&
+           reinterpret_cast<uintptr_t>(c.data) % 16 == 0;
+}
+
+// ---------------------------------------------------------------------------
+// Tiled FP32-form kernels (cell-sorted particles, one 128-thread CTA per work
+// item of the bins)
+// ---------------------------------------------------------------------------
+// Placement inside a tile: the spline of the plain FP32 form and the stencil
+// in tile-local node indices; false if the particle is not in this tile.
+template <int ORDER>
+struct TilePlace {
+    const MeshP& mp;
+    const TileP& tp;
+    const int* ob;
+    __device__ __forceinline__ bool operator()(const double xp[3], Spline1D<ORDER, float> sp[3],
+                                               int idx[3][SplineTraits<ORDER>::K]) const
+    {
+        int lb[3];
+        if (!locate<ORDER>(mp, tp, xp, ob, sp, lb)) return false;
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+#pragma unroll
+            for (int q = 0; q < SplineTraits<ORDER>::K; ++q) idx[d][q] = lb[d] + q;
+        return true;
+    }
+};
+
+__device__ __forceinline__ void count_unsorted(const TileP& tp, int64_t n, int* err)
+{
+    // particles sorted past the last tile (outside the mesh) belong to no item
+    if (blockIdx.x == 0 && threadIdx.x == 0 && err) {
+        const int64_t n_valid = __ldg(tp.off + tp.ntiles);
+        if (n > n_valid) atomicAdd(err, (int)(n - n_valid));
+    }
+}
+
+// P2G: the item's contributions are rounded to 64-bit fixed point exactly as
+// the plain kernel rounds them and summed in a shared-memory node tile with
+// 32-bit integer atomics on three slices of each value (q = hi 2^32 + mid
+// 2^16 + lo with mid, lo in [0, 2^16): the lo and mid sums of at most 65536
+// contributions are exact, the hi sum is exact modulo 2^32, so the
+// recombined 64-bit total equals the sum of the q modulo 2^64), then the tile
+// is added to the grid.  Integer sums do not depend on their order: the grid
+// is bit-identical to the plain kernel's (which adds every contribution to
+// the grid), with one grid atomic per touched node and field per item
+// instead of per particle and node.
+template <int ORDER, int NC>
+__global__ void __launch_bounds__(128)
+polypic_p2g_tiled_kernel(MeshP mp, TileP tp, int64_t n, PField x, PField m, PField u, PField c,
+                         GField gmu, GField gm, float dt, float scale_mu, float scale_m, int* err)
+{
+    extern __shared__ __align__(16) unsigned int pp_tacc[];  // 3 slices x (1 + NC) x nodes
+    count_unsorted(tp, n, err);
+    int64_t t, a, b;
+    if (!item_range(tp, blockIdx.x, t, a, b)) return;  // CTA-uniform
+    const int nodes = tp.nodes, slice = (1 + NC) * nodes;
+    for (int e = threadIdx.x; e < 3 * slice; e += blockDim.x) pp_tacc[e] = 0u;
+    __syncthreads();
+    int ob[3];
+    tile_origin(tp, t, ob);
+    const TilePlace<ORDER> place{mp, tp, ob};
+    for (int64_t p = a + threadIdx.x; p < b; p += blockDim.x)
+        polypic_p2g_particle<ORDER, NC, false, float, float>(
+            mp, p, x, m, u, dt, -1, err, place,
+            [&](int f, int i, int j, int k, float v) {
+                const long long q = __float2ll_rn(v * (f == 0 ? scale_m : scale_mu));
+                const int e = f * nodes + (i * tp.NT[1] + j) * tp.NT[2] + k;
+                atomicAdd(&pp_tacc[e], (unsigned int)(q & 0xFFFF));
+                atomicAdd(&pp_tacc[slice + e], (unsigned int)((q >> 16) & 0xFFFF));
+                atomicAdd(&pp_tacc[2 * slice + e], (unsigned int)(q >> 32));
+            },
+            [&](int v) { return c.get<float>(p, v); });
+    __syncthreads();
+    for (int e = threadIdx.x; e < nodes; e += blockDim.x) {
+        const int k = e % tp.NT[2], j = (e / tp.NT[2]) % tp.NT[1], i = e / (tp.NT[1] * tp.NT[2]);
+        const int gi = node_global(mp, tp, 0, ob[0], i);
+        const int gj = node_global(mp, tp, 1, ob[1], j);
+        const int gk = node_global(mp, tp, 2, ob[2], k);
+#pragma unroll
+        for (int f = 0; f <= NC; ++f) {
+            const int q = f * nodes + e;
+            const unsigned long long v = ((unsigned long long)pp_tacc[2 * slice + q] << 32) +
+                                         ((unsigned long long)pp_tacc[slice + q] << 16) +
+                                         (unsigned long long)pp_tacc[q];
+            if (v)
+                atomicAdd(reinterpret_cast<unsigned long long*>(
+                              f == 0 ? gm.ptr<long long>(gi, gj, gk, 0)
+                                     : gmu.ptr<long long>(gi, gj, gk, f - 1)),
+                          v);
+        }
+    }
+}
+
+// G2P: the tile's node velocities are staged once per item in shared memory;
+// packed c_p records leave through WarpRecords.
+template <int ORDER, int NC, bool WS>
+__global__ void __launch_bounds__(128)
+polypic_g2p_tiled_kernel(MeshP mp, TileP tp, int64_t n, PField x, GField u, PField c, int* err)
+{
+    extern __shared__ __align__(16) unsigned char pp_smem[];
+    float4* tile = reinterpret_cast<float4*>(pp_smem);
+    count_unsorted(tp, n, err);
+    int64_t t, a, b;
+    if (!item_range(tp, blockIdx.x, t, a, b)) return;  // CTA-uniform
+    int ob[3];
+    tile_origin(tp, t, ob);
+    for (int e = threadIdx.x; e < tp.nodes; e += blockDim.x) {
+        const int k = e % tp.NT[2], j = (e / tp.NT[2]) % tp.NT[1], i = e / (tp.NT[1] * tp.NT[2]);
+        const int gi = node_global(mp, tp, 0, ob[0], i);
+        const int gj = node_global(mp, tp, 1, ob[1], j);
+        const int gk = node_global(mp, tp, 2, ob[2], k);
+        const bool inside = (mp.periodic[0] || gi < mp.ext[0]) &&
+                            (mp.periodic[1] || gj < mp.ext[1]) &&
+                            (mp.periodic[2] || gk < mp.ext[2]);
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (inside) {
+            v.x = __ldg(u.ptr<float>(gi, gj, gk, 0));
+            if (NC > 1) v.y = __ldg(u.ptr<float>(gi, gj, gk, 1));
+            if (NC > 2) v.z = __ldg(u.ptr<float>(gi, gj, gk, 2));
+        }
+        tile[e] = v;
+    }
+    __syncthreads();
+    const TilePlace<ORDER> place{mp, tp, ob};
+    auto grid = [&](int i, int j, int k, int cc) {
+        const float4 v = tile[(i * tp.NT[1] + j) * tp.NT[2] + k];
+        return cc == 0 ? v.x : (cc == 1 ? v.y : v.z);
+    };
+    if constexpr (!WS) {
+        for (int64_t p = a + threadIdx.x; p < b; p += blockDim.x)
+            polypic_g2p_particle<ORDER, NC, false, float, float>(
+                mp, p, x, -1, err, place, grid, [&](int v, float val) { c.set<float>(p, v, val); });
+    } else {
+        constexpr int NV = PPModes<ORDER>::value * NC;
+        const int lane = threadIdx.x & 31;
+        const WarpRecords<float, NV> rec{
+            reinterpret_cast<float*>(pp_smem + ((sizeof(float4) * tp.nodes + 15) & ~size_t(15))) +
+            (threadIdx.x >> 5) * 32 * WarpRecords<float, NV>::NVP};
+        float* cbase = reinterpret_cast<float*>(c.data);
+        for (int64_t p0 = a + (threadIdx.x & ~31); p0 < b; p0 += blockDim.x) {
+            const int cnt = (int)min((int64_t)32, b - p0);
+            bool wrote = false;
+            if (lane < cnt)
+                wrote = polypic_g2p_particle<ORDER, NC, false, float, float>(
+                    mp, p0 + lane, x, -1, err, place, grid,
+                    [&](int v, float val) { rec.at(lane, v) = val; });
+            rec.store(cbase + p0 * NV, cnt, __ballot_sync(0xFFFFFFFFu, wrote), lane);
+        }
+    }
+}
+
+template <int ORDER, int NC>
+static picasso_status launch_pp_p2g_tiled(const MeshP& mp, const TileP& tp, int64_t n,
+                                          const PField& x, const PField& m, const PField& u,
+                                          const PField& c, const GField& gmu, const GField& gm,
+                                          double dt, int* err, cudaStream_t st)
+{
+    const size_t smem = 3 * sizeof(unsigned int) * (1 + NC) * (size_t)tp.nodes;
+    auto kern = polypic_p2g_tiled_kernel<ORDER, NC>;
+    PB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int64_t items = tp.ntiles + (n + tp.chunk - 1) / tp.chunk;
+    kern<<<(unsigned)items, 128, smem, st>>>(mp, tp, n, x, m, u, c, gmu, gm, (float)dt,
+                                             ldexpf(1.f, gmu.fixed_bits), ldexpf(1.f, gm.fixed_bits),
+                                             err);
+    return check_launch();
+}
+
+template <int ORDER, int NC>
+static picasso_status launch_pp_g2p_tiled(const MeshP& mp, const TileP& tp, int64_t n,
+                                          const PField& x, const GField& u, const PField& c,
+                                          int* err, cudaStream_t st)
+{
+    constexpr int NV = PPModes<ORDER>::value * NC;
+    const bool ws = packed_record<ORDER, NC, float>(c);
+    const size_t smem = ((sizeof(float4) * tp.nodes + 15) & ~size_t(15)) +
+                        (ws ? 4 * WarpRecords<float, NV>::kBytesPerWarp : 0);
+    const int64_t items = tp.ntiles + (n + tp.chunk - 1) / tp.chunk;
+    if (ws) {
+        auto kern = polypic_g2p_tiled_kernel<ORDER, NC, true>;
+        PB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kern<<<(unsigned)items, 128, smem, st>>>(mp, tp, n, x, u, c, err);
+    } else {
+        auto kern = polypic_g2p_tiled_kernel<ORDER, NC, false>;
+        PB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kern<<<(unsigned)items, 128, smem, st>>>(mp, tp, n, x, u, c, err);
+    }
+    return check_launch();
 }
 
 // ---------------------------------------------------------------------------
 // dispatch
 // ---------------------------------------------------------------------------
+// Launches `kernel` with warp-staged records (dynamic shared memory of four
+// warps' records) or without.
+template <class PT, int NV, class Kern, class... Args>
+static void launch_staged(Kern kernel, bool ws, unsigned blocks, cudaStream_t st, Args... args)
+{
+    const size_t smem = ws ? 4 * WarpRecords<PT, NV>::kBytesPerWarp : 0;
+    if (ws) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    kernel<<<blocks, 128, smem, st>>>(args...);
+}
+
+template <int ORDER, int NC, bool STAG, class PT, class R, class ACC>
+static void launch_pp_p2g_form(const MeshP& mp, int64_t n, const PField& x, const PField& m,
+                               const PField& u, const PField& c, const GField& gmu,
+                               const GField& gm, R dt, int col, R smu, R sm, int* err,
+                               cudaStream_t st)
+{
+    const unsigned blocks = grid_for(n, 128, 148LL * 128);
+    polypic_p2g_kernel<ORDER, NC, STAG, PT, R, ACC><<<blocks, 128, 0, st>>>(
+        mp, n, x, m, u, c, gmu, gm, dt, col, smu, sm, err);
+}
+
 template <int ORDER, int NC, bool STAG>
 static void launch_pp_p2g(int form, const MeshP& mp, int64_t n, const PField& x, const PField& m,
                           const PField& u, const PField& c, const GField& gmu, const GField& gm,
                           double dt, int col, int* err, cudaStream_t st)
 {
-    const int threads = 128;
-    const unsigned blocks = grid_for(n, threads, 148LL * 128);
     if (form == 0)
-        polypic_p2g_kernel<ORDER, NC, STAG, double, double, AccF64><<<blocks, threads, 0, st>>>(
-            mp, n, x, m, u, c, gmu, gm, dt, col, 0.0, 0.0, err);
+        launch_pp_p2g_form<ORDER, NC, STAG, double, double, AccF64>(
+            mp, n, x, m, u, c, gmu, gm, dt, col, 0.0, 0.0, err, st);
     else if (form == 1)
-        polypic_p2g_kernel<ORDER, NC, STAG, float, float, AccFixed><<<blocks, threads, 0, st>>>(
+        launch_pp_p2g_form<ORDER, NC, STAG, float, float, AccFixed>(
             mp, n, x, m, u, c, gmu, gm, (float)dt, col, ldexpf(1.0f, gmu.fixed_bits),
-            ldexpf(1.0f, gm.fixed_bits), err);
+            ldexpf(1.0f, gm.fixed_bits), err, st);
     else
-        polypic_p2g_kernel<ORDER, NC, STAG, double, double, AccFixed><<<blocks, threads, 0, st>>>(
+        launch_pp_p2g_form<ORDER, NC, STAG, double, double, AccFixed>(
             mp, n, x, m, u, c, gmu, gm, dt, col, ldexp(1.0, gmu.fixed_bits),
-            ldexp(1.0, gm.fixed_bits), err);
+            ldexp(1.0, gm.fixed_bits), err, st);
+}
+
+template <int ORDER, int NC, bool STAG, class T>
+static void launch_pp_g2p_form(const MeshP& mp, int64_t n, const PField& x, const GField& u,
+                               const PField& c, int col, int* err, cudaStream_t st)
+{
+    constexpr int NV = PPModes<ORDER>::value * NC;
+    const unsigned blocks = grid_for(n, 128, 148LL * 128);
+    if (!STAG && packed_record<ORDER, NC, T>(c))
+        launch_staged<T, NV>(polypic_g2p_kernel<ORDER, NC, STAG, T, T, T, true>, true, blocks, st,
+                             mp, n, x, u, c, col, err);
+    else
+        launch_staged<T, NV>(polypic_g2p_kernel<ORDER, NC, STAG, T, T, T, false>, false, blocks,
+                             st, mp, n, x, u, c, col, err);
 }
 
 template <int ORDER, int NC, bool STAG>
 static void launch_pp_g2p(bool f32, const MeshP& mp, int64_t n, const PField& x, const GField& u,
                           const PField& c, int col, int* err, cudaStream_t st)
 {
-    const int threads = 128;
-    const unsigned blocks = grid_for(n, threads, 148LL * 128);
-    if (f32)
-        polypic_g2p_kernel<ORDER, NC, STAG, float, float, float><<<blocks, threads, 0, st>>>(
-            mp, n, x, u, c, col, err);
-    else
-        polypic_g2p_kernel<ORDER, NC, STAG, double, double, double><<<blocks, threads, 0, st>>>(
-            mp, n, x, u, c, col, err);
+    if (f32) launch_pp_g2p_form<ORDER, NC, STAG, float>(mp, n, x, u, c, col, err, st);
+    else launch_pp_g2p_form<ORDER, NC, STAG, double>(mp, n, x, u, c, col, err, st);
 }
 
 #define PB_PP_NC_SWITCH(ncomp, ...)                                   \
@@ -365,6 +694,27 @@ static picasso_status polypic_common(const picasso_spline* sd, int64_t n, int32_
     // staggered: a 3-component field works on column `dim`, a scalar field
     // on column 0 (PolyPIC.hpp:181, :325)
     *col = (*stag >= 0) ? (ncomp == 3 ? *stag : 0) : -1;
+    return PICASSO_OK;
+}
+
+// Tiled path for sorted particles (picasso_exec.bins): FP32 form, collocated
+// locations; the bins must match the spline.  *tiled stays false (plain
+// kernels) when not eligible or when the node tile of `node_bytes` per node
+// does not fit in shared memory.
+static picasso_status polypic_tiles(const picasso_spline* sd, const picasso_exec* exec,
+                                    bool eligible, const MeshP& mp, int node_bytes, bool* tiled,
+                                    TileP* tp)
+{
+    *tiled = false;
+    if (!exec || !exec->bins) return PICASSO_OK;
+    if (exec->bins->order != sd->order || exec->bins->location != sd->location)
+        return PICASSO_ERR_INVALID_ARGUMENT;
+    if (!eligible) return PICASSO_OK;
+    if (!make_tilep(mp, sd->order, *exec->bins, tp)) return PICASSO_ERR_INVALID_ARGUMENT;
+    // records of four warps on top of the node tile in the G2P (at most)
+    const int64_t extra = 4 * 32 * 82 * 4;
+    if ((int64_t)node_bytes * tp->nodes + extra > device_smem_optin()) return PICASSO_OK;
+    *tiled = true;
     return PICASSO_OK;
 }
 
@@ -396,6 +746,21 @@ extern "C" picasso_status picasso_polypic_p2g(const picasso_spline* sd, int64_t 
     int* err = exec ? exec->error_count : nullptr;
     PField x = make_pfield(x_p), m = make_pfield(m_p), u = make_pfield(u_p), c = make_pfield(c_p);
     GField gmu = make_gfield(mu_i), gm = make_gfield(m_i);
+    bool tiled = false;
+    TileP tp;
+    // (the tile's 32-bit slice sums are exact for work items of at most
+    // 65536 particles)
+    const bool p2g_ok = form == 1 && stag < 0 && exec && exec->bins && exec->bins->chunk <= 65536;
+    if ((st = polypic_tiles(sd, exec, p2g_ok, mp, 12 * (1 + ncomp), &tiled, &tp))) return st;
+    if (tiled) {
+        if (sd->order == 1) {
+            PB_PP_NC_SWITCH(ncomp, return launch_pp_p2g_tiled<1, NC_>(mp, tp, num_particles, x, m,
+                                                                      u, c, gmu, gm, dt, err, s));
+        } else {
+            PB_PP_NC_SWITCH(ncomp, return launch_pp_p2g_tiled<2, NC_>(mp, tp, num_particles, x, m,
+                                                                      u, c, gmu, gm, dt, err, s));
+        }
+    }
     if (sd->order == 1) {
         if (stag >= 0) {
             PB_PP_NC_SWITCH(ncomp, launch_pp_p2g<1, NC_, true>(form, mp, num_particles, x, m, u, c,
@@ -429,6 +794,18 @@ extern "C" picasso_status picasso_polypic_g2p(const picasso_spline* sd, int64_t 
     int* err = exec ? exec->error_count : nullptr;
     PField x = make_pfield(x_p), c = make_pfield(c_p);
     GField u = make_gfield(u_i);
+    bool tiled = false;
+    TileP tp;
+    if ((st = polypic_tiles(sd, exec, f32 && stag < 0, mp, 16, &tiled, &tp))) return st;
+    if (tiled) {
+        if (sd->order == 1) {
+            PB_PP_NC_SWITCH(ncomp, return launch_pp_g2p_tiled<1, NC_>(mp, tp, num_particles, x, u,
+                                                                      c, err, s));
+        } else {
+            PB_PP_NC_SWITCH(ncomp, return launch_pp_g2p_tiled<2, NC_>(mp, tp, num_particles, x, u,
+                                                                      c, err, s));
+        }
+    }
     if (sd->order == 1) {
         if (stag >= 0) {
             PB_PP_NC_SWITCH(ncomp, launch_pp_g2p<1, NC_, true>(f32, mp, num_particles, x, u, c, col,

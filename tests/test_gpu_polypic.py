@@ -8,8 +8,9 @@ import torch
 
 import oracle
 from helpers import golden, poly_fill, reference_mesh, staggered_box_polypic, stencil_range
-from particles import periodic_mesh, rel_err, uniform_particles
-from picasso_b200 import FieldLocation, FixedGrid, PolyPIC, create_spline
+from particles import clustered_particles, periodic_mesh, rel_err, uniform_particles
+from picasso_b200 import (FieldLocation, FixedGrid, PolyPIC, UniformMesh, cell_sort, create_spline,
+                          permute_members)
 
 pytestmark = pytest.mark.gpu
 
@@ -167,3 +168,60 @@ def test_exact_recovery_single_particle(cuda, order):
     sel = gm > 0
     np.testing.assert_allclose(gmu[sel], gm[sel][:, None] * ug[sel], rtol=1e-10, atol=1e-12)
     assert sel.sum() == (order + 1) ** 3
+
+
+@pytest.mark.parametrize("order,layout,periodic", [(1, "packed", True), (2, "packed", True),
+                                                   (2, "strided", True), (2, "packed", False)])
+def test_tiled_fp32_form_equals_plain(cuda, order, layout, periodic):
+    """Cell-sorted particles with bins take the tiled FP32 kernels: the grid
+    (integer sums) and c_p must be the plain kernels' bits.  'strided': c_p
+    rows are not packed (the G2P writes records directly)."""
+    if periodic:
+        mesh = periodic_mesh(12, halo=0)
+        x, m, _ = clustered_particles(mesh, 12 ** 3 * 6, nblob=3, sigma_cells=1.5, frac=0.6,
+                                      seed=50 + order)
+    else:
+        mesh = UniformMesh([0, 0, 0, 1, 1, 1], cell_size=1 / 12, periodic=(False,) * 3,
+                           halo_cell_width=2)
+        x = np.random.default_rng(52).uniform(0.05, 0.95, (12 ** 3 * 6, 3))
+        m = np.random.default_rng(53).uniform(0.5, 1.5, x.shape[0])
+    nm = 8 if order == 1 else 27
+    u = _modes(np.random.default_rng(9), x.shape[0], nm, 3)
+    loc = FieldLocation.Node
+    ext = mesh.extent(loc)
+    dt = 0.1 * mesh.cell_size
+    f32 = torch.float32
+    xd, md, ud = _dev(x), _dev(m, f32), _dev(u, f32)
+    sd0 = create_spline(loc, order, mesh, xd)
+    _, perm, bins = cell_sort(sd0, (4, 4, 4), chunk=256)
+    xs, ms, us = permute_members(perm, xd, md, ud)
+    sd = create_spline(loc, order, mesh, xs)
+
+    def p2g(b):
+        gm = FixedGrid(torch.zeros(ext, dtype=torch.int64, device="cuda"), 36)
+        gmu = FixedGrid(torch.zeros(ext + (3,), dtype=torch.int64, device="cuda"), 36)
+        err = torch.zeros(1, dtype=torch.int32, device="cuda")
+        PolyPIC.p2g(ms, us, us, gmu, gm, dt, sd, bins=b, error_count=err)
+        torch.cuda.synchronize()
+        return gm.raw, gmu.raw, int(err.item())
+
+    gm_p, gmu_p, e_p = p2g(None)
+    gm_t, gmu_t, e_t = p2g(bins)
+    assert e_p == 0 and e_t == 0
+    assert bool((gm_t != 0).any())
+    assert torch.equal(gm_p, gm_t) and torch.equal(gmu_p, gmu_t)
+    g = torch.Generator(device="cuda").manual_seed(54)
+    ug = torch.randn(ext + (3,), generator=g, device="cuda", dtype=f32)
+
+    def g2p(b):
+        if layout == "packed":
+            c = torch.full((x.shape[0], nm, 3), 7.0, dtype=f32, device="cuda")
+        else:
+            c = torch.full((x.shape[0], nm + 1, 3), 7.0, dtype=f32, device="cuda")[:, :nm, :]
+        PolyPIC.g2p(ug, c, sd, bins=b)
+        torch.cuda.synchronize()
+        return c.clone()
+
+    c_p, c_t = g2p(None), g2p(bins)
+    assert not bool((c_t == 7.0).all())
+    assert torch.equal(c_p, c_t)
