@@ -26,14 +26,6 @@ __host__ __device__ __forceinline__ constexpr int mode_deg(int r, int d)
                   (2 * r)) & 3ull);
 }
 
-// Inverse of mode_deg: the mode with degrees (a, b, c) (all below D).
-__host__ __device__ __forceinline__ constexpr int mode_of(int a, int b, int c)
-{
-    int r = 0;
-    while (!(mode_deg(r, 0) == a && mode_deg(r, 1) == b && mode_deg(r, 2) == c)) ++r;
-    return r;
-}
-
 // a[i] for a register array and a run-time i (a select chain, no local memory).
 template <int K, class T>
 __device__ __forceinline__ T pick(const T (&a)[K], int i)
@@ -146,16 +138,13 @@ __device__ __forceinline__ void polypic_p2g_particle(const MeshP& mp, int64_t p,
 #pragma unroll 1
         for (int d0 = 0; d0 < NCU; d0 += CB) {
             R cp[D][D][D][CB];
+            // loop over the modes: their degrees fold to constants
 #pragma unroll
-            for (int a = 0; a < D; ++a)
+            for (int r = 0; r < D * D * D; ++r)
 #pragma unroll
-                for (int b = 0; b < D; ++b)
-#pragma unroll
-                    for (int cc = 0; cc < D; ++cc)
-#pragma unroll
-                        for (int e = 0; e < CB; ++e)
-                            cp[a][b][cc][e] =
-                                (R)mode(mode_of(a, b, cc) * ncp + (STAG ? col : d0 + e));
+                for (int e = 0; e < CB; ++e)
+                    cp[mode_deg(r, 0)][mode_deg(r, 1)][mode_deg(r, 2)][e] =
+                        (R)mode(r * ncp + (STAG ? col : d0 + e));
             // 27 FP64 modes: i-planes one after the other (not unrolled: bounds
             // the live range of the 9-node plane bodies, which would spill)
 #pragma unroll(sizeof(R) == 8 && ORDER == 2 ? 1 : K)
@@ -365,15 +354,11 @@ __device__ __forceinline__ bool polypic_g2p_particle(const MeshP& mp, int64_t p,
                                 cp[a][b][cc][e] += G[0][a][i] * t2[b][cc][e];
             }
 #pragma unroll
-            for (int a = 0; a < D; ++a)
+            for (int r = 0; r < D * D * D; ++r)
 #pragma unroll
-                for (int b = 0; b < D; ++b)
-#pragma unroll
-                    for (int cc = 0; cc < D; ++cc)
-#pragma unroll
-                        for (int e = 0; e < CB; ++e)
-                            emit(mode_of(a, b, cc) * ncp + (STAG ? col : d0 + e),
-                                 (PT)cp[a][b][cc][e]);
+                for (int e = 0; e < CB; ++e)
+                    emit(r * ncp + (STAG ? col : d0 + e),
+                         (PT)cp[mode_deg(r, 0)][mode_deg(r, 1)][mode_deg(r, 2)][e]);
         }
     }
     return true;
