@@ -464,7 +464,16 @@ polypic_p2g_tiled_kernel(MeshP mp, TileP tp, int64_t n, PField x, PField m, PFie
     int ob[3];
     tile_origin(tp, t, ob);
     const TilePlace<ORDER> place{mp, tp, ob};
-    for (int64_t p = a + threadIdx.x; p < b; p += blockDim.x)
+    // Quadratic: each thread sweeps its own contiguous run of the item, so
+    // that the lanes of a warp sit in different cells and their tile atomics
+    // rarely hit the same node (128^3 8 ppc: 6.5 ms instead of 9.1 ms with
+    // consecutive particles per warp).  Linear (8 nodes, little arithmetic)
+    // keeps consecutive particles per warp for coalesced loads (2.1 vs 2.5 ms).
+    const int64_t U = ORDER == 2 ? (b - a + blockDim.x - 1) / blockDim.x : 1;
+    const int64_t r0 = ORDER == 2 ? a + (int64_t)threadIdx.x * U : a + threadIdx.x;
+    const int64_t r1 = ORDER == 2 ? min(r0 + U, b) : b;
+    const int64_t step = ORDER == 2 ? 1 : blockDim.x;
+    for (int64_t p = r0; p < r1; p += step)
         polypic_p2g_particle<ORDER, NC, false, float, float>(
             mp, p, x, m, u, dt, -1, err, place,
             [&](int f, int i, int j, int k, float v) {
