@@ -696,7 +696,10 @@ def run_e2e(step, x, m32, c32, args, stream, dist, world):
     hc.copy_(c32)
     h2d = hx.numel() * 8 + hm.numel() * 4 + hc.numel() * 4
     d2h = houts[0].numel() * 4
-    steps = max(2, min(args.steps, 4))
+    # all K steps (not a shorter sample): the last result's device -> host
+    # copy drains after the last step and is part of the timed region, so
+    # fewer steps would overstate its share of a long run
+    steps = max(2, args.steps)
     s_in, s_run, s_out = torch.cuda.Stream(), stream, torch.cuda.Stream()
     # a second buffer set: positions, members and grids of its own, same bins
     other = Step(step.form, step.mesh, torch.empty_like(x), torch.empty_like(m32),
