@@ -385,6 +385,36 @@ PICASSO_API picasso_status picasso_cell_sort_static(const picasso_spline* sd,
                                                     picasso_bins* bins_out,
                                                     const picasso_exec* exec);
 
+/* Fastest launch knobs of the sorted (tiled) step for one instance. */
+typedef struct picasso_tune_result {
+    int32_t tile[3];   /* bins per tile for picasso_cell_sort */
+    int32_t chunk;     /* particles per work item */
+    int32_t p2g_lanes; /* picasso_bins.p2g_lanes */
+    float step_ms;     /* measured fill + P2G + velocity + G2P, milliseconds */
+} picasso_tune_result;
+
+/* Autotuner of the precision-form tiled step (FP32 m_p / c_p, 64-bit
+ * fixed-point m_i / mu_i, FP32 u_i; collocated, 3 components) on the
+ * caller's own particles: for tiles (4,4,4) (4,4,8) (4,8,8) (8,8,8), work items
+ * of 1024 and 4096 particles and 1 or 2 P2G lanes per particle (4 for cubic)
+ * it sorts and permutes copies of the particles and times `trials` steps of
+ * grid fill -> P2G -> grid velocity -> G2P with CUDA events on the stream,
+ * and writes the fastest candidate to *best.  The particle members are not
+ * modified; m_i, mu_i and u_i serve as the step's grids and hold the last
+ * candidate's values afterwards.  Allocates and frees device memory (about
+ * 84 bytes per particle plus the sort workspace) and waits for the stream:
+ * a set-up call, not one for a time step.  The candidates' grid results
+ * agree to FP32 rounding (the tiled P2G sums a work item in FP32 before its
+ * fixed-point flush, so the tiling sets the rounding; each choice is itself
+ * deterministic).  Returns PICASSO_ERR_UNSUPPORTED for staggered locations.  No reference
+ * counterpart (Picasso has no tiled path to tune). */
+PICASSO_API picasso_status picasso_autotune(const picasso_spline* sd, int64_t num_particles,
+                                            picasso_particle_field x_p, picasso_particle_field m_p,
+                                            picasso_particle_field c_p, picasso_grid_field m_i,
+                                            picasso_grid_field mu_i, picasso_grid_field u_i,
+                                            double mass_threshold, int32_t trials,
+                                            picasso_tune_result* best, const picasso_exec* exec);
+
 /* Gather a particle member: dst(p, c) = src(perm[p], c) for c < ncomp.
  * src and dst must not overlap. */
 PICASSO_API picasso_status picasso_permute(int64_t num_particles, int32_t ncomp, const uint32_t* perm,

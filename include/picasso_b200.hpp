@@ -349,6 +349,25 @@ inline void gridUpdate(const picasso_mesh& mesh, const GridArray& m_i, const Gri
           "gridUpdate");
 }
 
+// Launch knobs of the precision-form tiled step measured on the particles of
+// sd (picasso_autotune): tile and chunk for picasso_cell_sort, p2g_lanes for
+// the bins.  A set-up call: it allocates device memory and waits for the
+// stream; m_i / mu_i / u_i serve as the step's grids.
+template <class Location, class Order>
+picasso_tune_result autotune(const SplineData<Location, Order>& sd, const ParticleMember& m_p,
+                             const ParticleMember& c_p, const GridArray& m_i,
+                             const GridArray& mu_i, const GridArray& u_i,
+                             double mass_threshold = 1e-12, int32_t trials = 3,
+                             const Exec& ex = Exec())
+{
+    picasso_tune_result r{};
+    check(picasso_autotune(&sd.spline, sd.num_particles(), sd.x.field, m_p.field, c_p.field,
+                           m_i.field, mu_i.field, u_i.field, mass_threshold, trials, &r,
+                           &ex.exec),
+          "autotune");
+    return r;
+}
+
 // Many independent APIC problems stepped together (picasso_batch_*); owns the
 // batch handle.
 class Batch {

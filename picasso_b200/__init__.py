@@ -21,6 +21,7 @@ from .api import (  # noqa: F401
     Spline,
     UniformMesh,
     advect,
+    autotune,
     cell_sort,
     create_spline,
     fixed_bits_for,

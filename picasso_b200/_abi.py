@@ -89,6 +89,11 @@ class BatchInfo(C.Structure):
 
 BATCH_FUSED, BATCH_PHASED = 0, 1
 
+
+class TuneResult(C.Structure):
+    _fields_ = [("tile", C.c_int32 * 3), ("chunk", C.c_int32), ("p2g_lanes", C.c_int32),
+                ("step_ms", C.c_float)]
+
 # (name, restype, argtypes) of every entry point in the header
 SIGNATURES = [
     ("picasso_version", C.c_char_p, []),
@@ -135,6 +140,9 @@ SIGNATURES = [
     ("picasso_cell_sort_static", C.c_int,
      [C.POINTER(Spline), C.c_int64, ParticleField, C.POINTER(C.c_int32), C.c_int32, C.c_void_p,
       C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(Bins), C.POINTER(Exec)]),
+    ("picasso_autotune", C.c_int,
+     [C.POINTER(Spline), C.c_int64, ParticleField, ParticleField, ParticleField, GridField,
+      GridField, GridField, C.c_double, C.c_int32, C.POINTER(TuneResult), C.POINTER(Exec)]),
     ("picasso_permute", C.c_int,
      [C.c_int64, C.c_int32, C.c_void_p, ParticleField, ParticleField, C.POINTER(Exec)]),
     ("picasso_mat3_inverse", C.c_int,

@@ -510,6 +510,23 @@ def permute_members(perm, *members, stream=None):
     return tuple(permute(perm, m, stream=stream) for m in members)
 
 
+def autotune(sd, m_p, c_p, m_i, mu_i, u_i, mass_threshold=1e-12, trials=3, stream=None):
+    """Launch knobs of the precision-form tiled step measured on these
+    particles (picasso_autotune): returns {"tile", "chunk", "p2g_lanes",
+    "step_ms"}.  The particle tensors are not modified; m_i, mu_i (FixedGrid)
+    and u_i (FP32) serve as the step's grids.  Allocates device memory and
+    waits for the stream: call it at set-up, then pass tile / chunk to
+    cell_sort and p2g_lanes to it (or to the bins)."""
+    res = _abi.TuneResult()
+    ex = _exec(stream, None, None)
+    check(_lib().picasso_autotune(C.byref(sd.desc), sd.num_particles, particle_field(sd.x),
+                                  particle_field(m_p), particle_field(c_p), grid_field(m_i),
+                                  grid_field(mu_i), grid_field(u_i), float(mass_threshold),
+                                  int(trials), C.byref(res), C.byref(ex.desc)), "autotune")
+    return {"tile": tuple(res.tile), "chunk": res.chunk, "p2g_lanes": res.p2g_lanes,
+            "step_ms": res.step_ms}
+
+
 # ---------------------------------------------------------------------------
 # 3x3 linear algebra
 # ---------------------------------------------------------------------------

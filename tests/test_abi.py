@@ -56,6 +56,7 @@ def test_descriptor_layout_matches_ctypes(tmp_path):
                                                         "error_count"]),
         "picasso_batch_info": (_abi.BatchInfo, ["count", "precision_form", "grid_blocks",
                                                 "smem_bytes", "items", "particles"]),
+        "picasso_tune_result": (_abi.TuneResult, ["tile", "chunk", "p2g_lanes", "step_ms"]),
     }
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "picasso_b200.h"',
              "int main(void) {"]
@@ -198,6 +199,25 @@ def test_sort_keys_and_key_emission_reject_on_host():
     assert lib.picasso_apic_g2p_advect_keys(C.byref(sp), 10, x, u, c, 0.1, tile, None,
                                             None) == _abi.ERR_INVALID_ARGUMENT
     assert lib.picasso_apic_g2p_advect_keys(C.byref(sp), 0, x, u, c, 0.1, tile, None, None) == 0
+
+
+def test_autotune_rejects_on_host():
+    lib = _abi.load_library()
+    sp = _spline(n=16)
+    x, m, c = _pf(), _pf(_abi.F32), _pf(_abi.F32)
+    m.tile_stride, c.tile_stride = 1, 12
+    gm, gmu, gu = _gf(_abi.I64_FIXED), _gf(_abi.I64_FIXED), _gf(_abi.F32)
+    gm.fixed_bits = gmu.fixed_bits = 36
+    res = _abi.TuneResult()
+
+    def tune(n=100, trials=3, out=True, mm=m, spl=sp):
+        return lib.picasso_autotune(C.byref(spl), n, x, mm, c, gm, gmu, gu, 1e-12, trials,
+                                    C.byref(res) if out else None, None)
+    assert tune(out=False) == _abi.ERR_INVALID_ARGUMENT
+    assert tune(n=0) == _abi.ERR_INVALID_ARGUMENT
+    assert tune(trials=0) == _abi.ERR_INVALID_ARGUMENT
+    assert tune(mm=_pf(_abi.F64)) == _abi.ERR_INVALID_ARGUMENT  # the FP32 form only
+    assert tune(spl=_spline(location=_abi.FACE_I, n=16)) == _abi.ERR_UNSUPPORTED
 
 
 def _batch_instance(f32=True):

@@ -57,6 +57,8 @@ int main(int argc, char**) {
         B200::gridUpdate(mesh, u, u, u, prm, u);
         B200::Batch batch(nullptr, 0);
         batch.step();
+        picasso_tune_result tr = B200::autotune(sd, m, c, u, u, u);
+        (void)tr;
         B200::FieldManager fm;
         fm.setMesh(FieldLocation::Node(), mesh);
         fm.add(FieldLocation::Node(), GV(), u);
