@@ -21,7 +21,6 @@ from .api import (  # noqa: F401
     Spline,
     UniformMesh,
     advect,
-    autotune,
     cell_sort,
     create_spline,
     fixed_bits_for,
@@ -33,6 +32,7 @@ from .api import (  # noqa: F401
     particle_field,
     permute,
     permute_members,
+    tune_tiled_step,
 )
 
 __version__ = "0.1.0"

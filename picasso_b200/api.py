@@ -510,7 +510,7 @@ def permute_members(perm, *members, stream=None):
     return tuple(permute(perm, m, stream=stream) for m in members)
 
 
-def autotune(sd, m_p, c_p, m_i, mu_i, u_i, mass_threshold=1e-12, trials=3, stream=None):
+def tune_tiled_step(sd, m_p, c_p, m_i, mu_i, u_i, mass_threshold=1e-12, trials=3, stream=None):
     """Launch knobs of the precision-form tiled step measured on these
     particles (picasso_autotune): returns {"tile", "chunk", "p2g_lanes",
     "step_ms"}.  The particle tensors are not modified; m_i, mu_i (FixedGrid)

@@ -269,3 +269,12 @@ def test_batch_create_rejects_invalid_instances_on_host(case):
     st = lib.picasso_batch_create(insts, count, mode, out_ptr)
     assert st == _abi.ERR_INVALID_ARGUMENT
     assert not out.value
+
+
+def test_package_names():
+    """The tuner module and the native tuner's wrapper are both reachable
+    (the wrapper must not shadow the module)."""
+    import picasso_b200 as pb
+    from picasso_b200 import autotune
+    assert hasattr(autotune, "Tuner")
+    assert callable(pb.tune_tiled_step)

@@ -9,8 +9,8 @@ import pytest
 import torch
 
 from particles import clustered_particles, periodic_mesh
-from picasso_b200 import (APIC, FieldLocation, FixedGrid, autotune, cell_sort, create_spline,
-                          permute_members)
+from picasso_b200 import (APIC, FieldLocation, FixedGrid, cell_sort, create_spline,
+                          permute_members, tune_tiled_step)
 
 pytestmark = pytest.mark.gpu
 N = 16
@@ -46,7 +46,7 @@ def test_autotune_choice_is_a_candidate_and_exact(cuda, order):
     x0, m0, c0 = xd.clone(), md.clone(), cd.clone()
     sd = create_spline(FieldLocation.Node, order, mesh, xd)
     _, gm, gmu, u = _grids(mesh.extent(FieldLocation.Node))
-    r = autotune(sd, md, cd, gm, gmu, u, trials=2)
+    r = tune_tiled_step(sd, md, cd, gm, gmu, u, trials=2)
     assert r["tile"] in TILES and r["chunk"] in (1024, 4096)
     assert r["p2g_lanes"] in ((4,) if order == 3 else (1, 2))
     assert r["step_ms"] > 0.0
