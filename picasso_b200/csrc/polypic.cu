@@ -207,23 +207,14 @@ struct PPModes {
 
 // Shared-memory records of a warp's 32 consecutive particles (packed c_p of
 // NV values each, at an odd stride so that the 32 lanes' records start on
-// distinct banks): the record of every particle is read or written by the
-// warp with coalesced accesses instead of NV strided accesses per thread.
+// distinct banks): the warp writes every particle's record with coalesced
+// stores instead of NV strided stores per thread.
 template <class PT, int NV>
 struct WarpRecords {
     static constexpr int NVP = NV | 1;
     PT* buf;
     static constexpr size_t kBytesPerWarp = sizeof(PT) * 32 * NVP;
     __device__ __forceinline__ PT& at(int lane, int v) const { return buf[lane * NVP + v]; }
-    // records of particles p0 .. p0 + cnt - 1 from packed storage
-    __device__ __forceinline__ void load(const PT* src, int cnt, int lane) const
-    {
-        for (int e = lane; e < cnt * NV; e += 32) {
-            const int q = e / NV;
-            buf[q * NVP + (e - q * NV)] = __ldg(src + e);
-        }
-        __syncwarp();
-    }
     // records of the particles in `mask` (bit q: particle p0 + q) to packed
     // storage
     __device__ __forceinline__ void store(PT* dst, int cnt, unsigned mask, int lane) const
@@ -366,7 +357,9 @@ __device__ __forceinline__ bool polypic_g2p_particle(const MeshP& mp, int64_t p,
     return true;
 }
 
-// WS: c_p is packed and written through WarpRecords (see polypic_p2g_kernel).
+// WS: c_p is packed (the record of particle p at element p * NV) and written
+// through WarpRecords; the lanes of a warp take consecutive particles and
+// iterate together.
 template <int ORDER, int NC, bool STAG, class GT, class PT, class R, bool WS>
 __global__ void __launch_bounds__(128)
 polypic_g2p_kernel(MeshP mp, int64_t n, PField x, GField u, PField c, int col, int* err)
