@@ -515,6 +515,10 @@ def run_advect(args, peak):
         state = {"x": x, "m": m, "c": c, "keys": None}
         keybuf = torch.empty(n, dtype=torch.int32, device="cuda")
         tile = tuple(args.adv_tile)
+        # the permutation writes into the other one of two member sets, so the
+        # timed steps allocate no particle storage
+        spare = {"x": torch.empty_like(x), "m": torch.empty_like(m), "c": torch.empty_like(c)}
+        sort_ws = pb.api.sort_workspace(pb.create_spline(loc, 3, mesh, x), tile)
 
         def step(ev=None):
             def mark(i):
@@ -523,10 +527,11 @@ def run_advect(args, peak):
             mark(0)
             sd0 = pb.create_spline(loc, 3, mesh, state["x"])
             _, perm, bins = pb.cell_sort(sd0, tile, chunk=4096, p2g_lanes=4 if f32 else 0,
-                                         keys=state["keys"])
+                                         keys=state["keys"], workspace=sort_ws)
             mark(1)
-            state["x"], state["m"], state["c"] = pb.permute_members(
-                perm, state["x"], state["m"], state["c"])
+            for name in ("x", "m", "c"):
+                pb.permute(perm, state[name], spare[name])
+                state[name], spare[name] = spare[name], state[name]
             mark(2)
             sd = pb.create_spline(loc, 3, mesh, state["x"])
             pb.grid_fill(desc, fill, 0.0, ncomp=4)
@@ -558,7 +563,7 @@ def run_advect(args, peak):
                      "transfer_ms": per["fill"] + per["p2g"] + per["velocity"]
                      + per["g2p_advect"], "kernels_ms": per,
                      "positions_in_box": bool(float(xs.min()) >= 0.0 and float(xs.max()) < 1.0)}
-        del state, x, m, c, acc, u, keybuf
+        del state, spare, x, m, c, acc, u, keybuf, sort_ws
         torch.cuda.synchronize()
         torch.cuda.empty_cache()
     res["speedup_fp32_vs_fp64"] = res["fp64"]["ms_per_step"] / res["fp32"]["ms_per_step"]

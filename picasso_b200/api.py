@@ -493,6 +493,16 @@ def cell_sort(sd, tile=(4, 8, 8), chunk=4096, stream=None, workspace=None, p2g_l
     return key[:n], perm[:n], Bins(bins, tile_offset, tile_items)
 
 
+def sort_workspace(sd, tile=(4, 8, 8)):
+    """Device workspace for cell_sort(sd, tile, workspace=...), to keep one
+    across steps instead of allocating it in every call."""
+    t3 = (C.c_int32 * 3)(*tile)
+    nbytes = C.c_int64()
+    check(_lib().picasso_cell_sort_workspace(C.byref(sd.desc), sd.num_particles, t3,
+                                             C.byref(nbytes)), "cell_sort_workspace")
+    return torch.empty(max(nbytes.value, 1), dtype=torch.uint8, device=sd.x.device)
+
+
 def permute(perm, src, dst=None, stream=None):
     """dst[p] = src[perm[p]] for a particle member tensor."""
     if dst is None:

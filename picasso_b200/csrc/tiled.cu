@@ -11,7 +11,13 @@
 
 namespace pb {
 
-constexpr int kG2PThreads = 128;
+// Threads of a tiled G2P CTA (one work item each).  Measured at 256^3
+// 8 ppc: quadratic 2.92 ms with 128 threads, 2.79 with 64, 2.94 with 32;
+// cubic 5.09 / 4.73 / 4.54 ms; linear 1.87 with 64, 2.28 with 32.
+template <int ORDER>
+struct G2PThreads {
+    static constexpr int value = ORDER == 3 ? 32 : 64;
+};
 
 template <int ORDER, int LPP>
 __global__ void __launch_bounds__(32, (P2GOccupancy<ORDER, LPP>::value))
@@ -29,7 +35,7 @@ p2g_tiled_kernel(P2GArgs A, int64_t n)
 }
 
 template <int ORDER, bool ADV>
-__global__ void __launch_bounds__(kG2PThreads) g2p_tiled_kernel(G2PArgs A, int64_t n)
+__global__ void __launch_bounds__(G2PThreads<ORDER>::value) g2p_tiled_kernel(G2PArgs A, int64_t n)
 {
     extern __shared__ __align__(16) float smem[];
     if (blockIdx.x == 0 && threadIdx.x == 0 && A.err) {
@@ -38,7 +44,8 @@ __global__ void __launch_bounds__(kG2PThreads) g2p_tiled_kernel(G2PArgs A, int64
     }
     int64_t t, a, b;
     if (!item_range(A.tp, blockIdx.x, t, a, b)) return;  // CTA-uniform
-    g2p_item<ORDER, kG2PThreads, ADV>(A, t, a, b, reinterpret_cast<float4*>(smem), threadIdx.x);
+    g2p_item<ORDER, G2PThreads<ORDER>::value, ADV>(A, t, a, b, reinterpret_cast<float4*>(smem),
+                                                  threadIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -244,7 +251,8 @@ static picasso_status launch_g2p_tiled(const G2PArgs& A, int64_t n, cudaStream_t
     PB_CUDA_TRY(cudaFuncSetAttribute(g2p_tiled_kernel<ORDER, ADV>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int64_t items = item_bound(A.tp, n);
-    g2p_tiled_kernel<ORDER, ADV><<<(unsigned)(items ? items : 1), kG2PThreads, smem, st>>>(A, n);
+    g2p_tiled_kernel<ORDER, ADV>
+        <<<(unsigned)(items ? items : 1), G2PThreads<ORDER>::value, smem, st>>>(A, n);
     return check_launch();
 }
 
