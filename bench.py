@@ -143,10 +143,12 @@ class Clocks:
 # ---------------------------------------------------------------------------
 # reference arm: the oracle port of the reference's CPU path
 # ---------------------------------------------------------------------------
-def cpu_sample(args, steps, warmup, nthreads):
+def cpu_sample(args, steps, warmup, nthreads, check_gpu=False):
     """P2G -> velocity -> G2P of the CPU port (OpenMP, duplicated scatter
     grids as Kokkos' OpenMP ScatterView) on a bounded sample: the same
-    workload generator on a grid^3 periodic box (grid = --cpu-sample-grid)."""
+    workload generator on a grid^3 periodic box (grid = --cpu-sample-grid).
+    check_gpu: the GPU forms then run the same step on the same particles
+    and their errors against this FP64 result are returned as well."""
     import numpy as np
     import torch
 
@@ -163,16 +165,94 @@ def cpu_sample(args, steps, warmup, nthreads):
     for s in range(warmup + steps):
         cc = c.copy()
         t0 = time.perf_counter()
-        oracle.apic_step_omp(sd, x, m, cc, nthreads)
+        grids = oracle.apic_step_omp(sd, x, m, cc, nthreads)
         t1 = time.perf_counter()
         if s >= warmup:
             times.append(t1 - t0)
     sec = sum(times) / len(times)
-    return {"value": x.shape[0] / sec, "unit": "particles/s", "cores": nthreads, "kind": "port",
-            "sample": "%d^3 periodic grid, %d ppc (%d particles), order %d, %s positions, "
-                      "FP64, OpenMP with duplicated scatter grids; mean of %d steps"
-                      % (n, args.ppc, x.shape[0], args.order, args.workload, steps),
-            "ms_per_step": 1e3 * sec}
+    out = {"value": x.shape[0] / sec, "unit": "particles/s", "cores": nthreads, "kind": "port",
+           "sample": "%d^3 periodic grid, %d ppc (%d particles), order %d, %s positions, "
+                     "FP64, OpenMP with duplicated scatter grids; mean of %d steps"
+                     % (n, args.ppc, x.shape[0], args.order, args.workload, steps),
+           "ms_per_step": 1e3 * sec}
+    if check_gpu:
+        out["errors_vs_oracle"] = gpu_errors_vs_oracle(args, mesh, x, m, c, grids, cc)
+    return out
+
+
+def _errs(got, ref, mask=None):
+    """normwise max|a-b|/max|b| and the largest per-entry relative error (per
+    grid node with m > threshold, or per particle: max-norm over components)."""
+    import numpy as np
+    got = np.asarray(got, dtype=np.float64)
+    ref = np.asarray(ref, dtype=np.float64)
+    den = np.abs(ref).max()
+    nw = float(np.abs(got - ref).max() / den) if den > 0 else 0.0
+    axes = tuple(range(mask.ndim if mask is not None else 1, ref.ndim))
+    num = np.abs(got - ref).max(axis=axes) if axes else np.abs(got - ref)
+    dd = np.abs(ref).max(axis=axes) if axes else np.abs(ref)
+    sel = dd > 0
+    if mask is not None:
+        sel &= mask
+    pe = float((num[sel] / dd[sel]).max()) if sel.any() else 0.0
+    return {"normwise": nw, "per_entry": pe}
+
+
+def gpu_errors_vs_oracle(args, mesh, x, m, c, grids, c_ref):
+    """Errors of the GPU forms against the oracle's FP64 step on the CPU
+    sample: FP32 form (tiled kernels on cell-sorted particles, the headline
+    path) and FP64 plain form (unsorted particles)."""
+    import torch
+
+    import picasso_b200 as pb
+
+    gm_o, gmu_o, gu_o = grids
+    heavy = gm_o > 1e-12
+    loc = pb.FieldLocation.Node
+    ext = mesh.extent(loc)
+    xd = torch.as_tensor(x, device="cuda")
+    res = {"sample": "the CPU-baseline sample (%d^3, %d ppc, %s, order %d); per_entry: per "
+                     "grid node with m > 1e-12 or per particle, max-norm over components"
+                     % (args.cpu_sample_grid, args.ppc, args.workload, args.order)}
+    # FP32 form, tiled (the headline path)
+    sd = pb.create_spline(loc, args.order, mesh, xd)
+    _, perm, bins = pb.cell_sort(sd, tuple(args.tile), chunk=args.chunk,
+                                 p2g_lanes=args.p2g_lanes)
+    xs, ms, cs = pb.permute_members(perm, xd, torch.as_tensor(m, dtype=torch.float32,
+                                                              device="cuda"),
+                                    torch.as_tensor(c, dtype=torch.float32,
+                                                    device="cuda").contiguous())
+    sds = pb.create_spline(loc, args.order, mesh, xs)
+    acc = torch.zeros(ext + (4,), dtype=torch.int64, device="cuda")
+    gm, gmu = pb.FixedGrid(acc[..., 0], FIXED_BITS), pb.FixedGrid(acc[..., 1:], FIXED_BITS)
+    u = torch.zeros(ext + (3,), dtype=torch.float32, device="cuda")
+    pb.APIC.p2g(ms, cs, gm, gmu, sds, bins=bins)
+    pb.grid_velocity(sds.desc.mesh, gm, gmu, u, 1e-12)
+    pb.APIC.g2p(u, cs, sds, bins=bins)
+    back = torch.empty_like(cs)
+    back[perm.long()] = cs
+    cb = back.double().cpu().numpy()
+    res["fp32_tiled"] = {"grid_mass": _errs(gm.to_float().cpu().numpy(), gm_o, heavy),
+                         "grid_momentum": _errs(gmu.to_float().cpu().numpy(), gmu_o, heavy),
+                         "grid_velocity": _errs(u.double().cpu().numpy(), gu_o, heavy),
+                         "particle_velocity": _errs(cb[:, 0], c_ref[:, 0]),
+                         "particle_affine": _errs(cb[:, 1:], c_ref[:, 1:])}
+    # FP64 plain form, unsorted
+    sd = pb.create_spline(loc, args.order, mesh, xd)
+    g64 = torch.zeros(ext + (4,), dtype=torch.float64, device="cuda")
+    u64 = torch.zeros(ext + (3,), dtype=torch.float64, device="cuda")
+    c64 = torch.as_tensor(c, device="cuda").clone()
+    pb.APIC.p2g(torch.as_tensor(m, device="cuda"), c64, g64[..., 0], g64[..., 1:], sd)
+    pb.grid_velocity(sd.desc.mesh, g64[..., 0], g64[..., 1:], u64, 1e-12)
+    pb.APIC.g2p(u64, c64, sd)
+    c64h = c64.cpu().numpy()
+    g64h = g64.cpu().numpy()
+    res["fp64_plain"] = {"grid_mass": _errs(g64h[..., 0], gm_o, heavy),
+                         "grid_momentum": _errs(g64h[..., 1:], gmu_o, heavy),
+                         "grid_velocity": _errs(u64.cpu().numpy(), gu_o, heavy),
+                         "particle_velocity": _errs(c64h[:, 0], c_ref[:, 0]),
+                         "particle_affine": _errs(c64h[:, 1:], c_ref[:, 1:])}
+    return res
 
 
 def run_reference(args):
@@ -426,8 +506,10 @@ def run_ours(args):
         legs["advect_cubic"] = run_advect(args, peak)
         legs["polypic"] = run_polypic(args, peak)
     cpu = None
+    errors_vs_oracle = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_sample(args, 3, 1, os.cpu_count() or 1)
+        cpu = cpu_sample(args, 3, 1, os.cpu_count() or 1, check_gpu=True)
+        errors_vs_oracle = cpu.get("errors_vs_oracle")
         cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
 
     ms32, per32, rf32, k32 = out["fp32"]
@@ -456,6 +538,8 @@ def run_ours(args):
         line["e2e"] = e2e
     if cpu:
         line["cpu_baseline"] = cpu
+    if errors_vs_oracle:
+        line["errors_vs_oracle"] = errors_vs_oracle
     line.update(legs)
     if rank == 0:
         print(json.dumps(line))
@@ -518,7 +602,7 @@ def run_advect(args, peak):
         # the permutation writes into the other one of two member sets, so the
         # timed steps allocate no particle storage
         spare = {"x": torch.empty_like(x), "m": torch.empty_like(m), "c": torch.empty_like(c)}
-        sort_ws = pb.api.sort_workspace(pb.create_spline(loc, 3, mesh, x), tile)
+        sort_bufs = pb.SortBuffers(pb.create_spline(loc, 3, mesh, x), tile)
 
         def step(ev=None):
             def mark(i):
@@ -527,7 +611,7 @@ def run_advect(args, peak):
             mark(0)
             sd0 = pb.create_spline(loc, 3, mesh, state["x"])
             _, perm, bins = pb.cell_sort(sd0, tile, chunk=4096, p2g_lanes=4 if f32 else 0,
-                                         keys=state["keys"], workspace=sort_ws)
+                                         keys=state["keys"], out=sort_bufs)
             mark(1)
             for name in ("x", "m", "c"):
                 pb.permute(perm, state[name], spare[name])
@@ -563,7 +647,7 @@ def run_advect(args, peak):
                      "transfer_ms": per["fill"] + per["p2g"] + per["velocity"]
                      + per["g2p_advect"], "kernels_ms": per,
                      "positions_in_box": bool(float(xs.min()) >= 0.0 and float(xs.max()) < 1.0)}
-        del state, spare, x, m, c, acc, u, keybuf, sort_ws
+        del state, spare, x, m, c, acc, u, keybuf, sort_bufs
         torch.cuda.synchronize()
         torch.cuda.empty_cache()
     res["speedup_fp32_vs_fp64"] = res["fp64"]["ms_per_step"] / res["fp32"]["ms_per_step"]

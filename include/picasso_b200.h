@@ -160,6 +160,13 @@ typedef struct picasso_exec {
     int32_t* error_count;   /* optional device int32: particles skipped because
                                their stencil left a non-periodic mesh */
     const picasso_bins* bins; /* optional: particles are tile-sorted (see above) */
+    int32_t* overflow_count;  /* optional device int32, I64_FIXED grids only: P2G
+                                 counts contributions (and tile sums) whose
+                                 |value| * 2^fixed_bits reached 2^62, the grid
+                                 velocity / update passes count nodes whose
+                                 mass sum wrapped negative; nonzero means the
+                                 fixed-point grid is unreliable (choose fewer
+                                 fraction bits) */
 } picasso_exec;
 
 /* ------------------------------------------------------------------------ */
@@ -371,11 +378,12 @@ PICASSO_API picasso_status picasso_cell_sort_keys(const picasso_spline* sd, int6
  * process exits.  Returns PICASSO_ERR_OUT_OF_RANGE, before any launch, when
  * the sort needs more than 32 MiB (picasso_cell_sort_workspace reports the
  * need; about 8 bytes per particle plus the digit tables, i.e. up to roughly
- * 3 million particles).  The first call on a device looks up the array's
- * device address (cudaGetSymbolAddress); make that first call before any
- * stream capture.  All calls share the array: calls whose work overlaps on the
- * GPU (other streams, other host threads) race, so order them.  No
- * counterpart in the reference. */
+ * 3 million particles).  Every call looks up the array's device address in
+ * the current context (cudaGetSymbolAddress), so a device or context reset in
+ * between is harmless; the first call on a device may load the module, so
+ * make it before any stream capture.  All calls share the array: calls whose
+ * work overlaps on the GPU (other streams, other host threads) race, so order
+ * them.  No counterpart in the reference. */
 PICASSO_API picasso_status picasso_cell_sort_static(const picasso_spline* sd,
                                                     int64_t num_particles,
                                                     picasso_particle_field x_p,
@@ -488,8 +496,8 @@ PICASSO_API picasso_status picasso_batch_create(const picasso_batch_instance* in
 /* One APIC step of every instance on `stream`.  use_graph != 0 replays a
  * CUDA graph captured at the first such call (one memset node + the
  * persistent launches).  Returns PICASSO_ERR_CUDA for launch errors; a wait
- * that ran out (which the design rules out) is reported by
- * picasso_batch_status.  Steps of one batch must not overlap on the GPU (they
+ * that ran out (which the queue order rules out at the default limit) is
+ * reported by picasso_batch_status.  Steps of one batch must not overlap on the GPU (they
  * share the queue counters). */
 PICASSO_API picasso_status picasso_batch_step(picasso_batch* batch, void* stream,
                                               int32_t use_graph);
@@ -498,8 +506,21 @@ PICASSO_API picasso_status picasso_batch_step(picasso_batch* batch, void* stream
  * picasso_apic_g2p): the comparison for the batched launch. */
 PICASSO_API picasso_status picasso_batch_step_sequential(picasso_batch* batch, void* stream);
 /* Synchronises `stream` and returns PICASSO_ERR_TIMEOUT if a dependency wait
- * of an earlier step ran out of polls (and clears that flag), else PICASSO_OK. */
+ * of an earlier step ran out of polls or gave up after picasso_batch_cancel
+ * (and clears the flag), else PICASSO_OK.  Items whose wait gave up skip
+ * their work, so that step's results are incomplete. */
 PICASSO_API picasso_status picasso_batch_status(picasso_batch* batch, void* stream);
+/* Bound of every dependency wait of the fused step, in polls of ~0.25 us
+ * (default 2^22, about a second).  Takes effect from the next step (a
+ * captured graph is released and captured again).  0 makes a wait give up at
+ * its first unmet check.  No counterpart in the reference. */
+PICASSO_API picasso_status picasso_batch_set_wait_limit(picasso_batch* batch, uint32_t polls);
+/* Enqueues on `stream` a write of the batch's status word: every dependency
+ * wait of a fused step that runs after it gives up at once (its item is
+ * skipped) until picasso_batch_status reads and clears the flag.  The host's
+ * way to end a fused step early, e.g. when another rank has failed.  No
+ * counterpart in the reference. */
+PICASSO_API picasso_status picasso_batch_cancel(picasso_batch* batch, void* stream);
 PICASSO_API picasso_status picasso_batch_get_info(const picasso_batch* batch,
                                                   picasso_batch_info* info);
 PICASSO_API picasso_status picasso_batch_destroy(picasso_batch* batch);

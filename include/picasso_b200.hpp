@@ -211,15 +211,16 @@ struct GridArray {
 };
 
 // Execution context: stream, optional skipped-particle counter, optional
-// sorted bins (see picasso_cell_sort).
+// sorted bins (see picasso_cell_sort), optional fixed-point overflow counter.
 struct Exec {
-    picasso_exec exec{nullptr, nullptr, nullptr};
+    picasso_exec exec{nullptr, nullptr, nullptr, nullptr};
     explicit Exec(void* stream = nullptr, int32_t* error_count = nullptr,
-                  const picasso_bins* bins = nullptr)
+                  const picasso_bins* bins = nullptr, int32_t* overflow_count = nullptr)
     {
         exec.stream = stream;
         exec.error_count = error_count;
         exec.bins = bins;
+        exec.overflow_count = overflow_count;
     }
 };
 

@@ -18,6 +18,7 @@ from .api import (  # noqa: F401
     FixedGrid,
     InterpolationOrder,
     PolyPIC,
+    SortBuffers,
     Spline,
     UniformMesh,
     advect,
@@ -32,6 +33,7 @@ from .api import (  # noqa: F401
     particle_field,
     permute,
     permute_members,
+    sort_workspace,
     tune_tiled_step,
 )
 

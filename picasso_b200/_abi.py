@@ -63,7 +63,7 @@ class Bins(C.Structure):
 
 class Exec(C.Structure):
     _fields_ = [("stream", C.c_void_p), ("error_count", C.c_void_p),
-                ("bins", C.POINTER(Bins))]
+                ("bins", C.POINTER(Bins)), ("overflow_count", C.c_void_p)]
 
 
 class GridUpdateParams(C.Structure):
@@ -153,6 +153,8 @@ SIGNATURES = [
     ("picasso_batch_step", C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
     ("picasso_batch_step_sequential", C.c_int, [C.c_void_p, C.c_void_p]),
     ("picasso_batch_status", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("picasso_batch_set_wait_limit", C.c_int, [C.c_void_p, C.c_uint32]),
+    ("picasso_batch_cancel", C.c_int, [C.c_void_p, C.c_void_p]),
     ("picasso_batch_get_info", C.c_int, [C.c_void_p, C.POINTER(BatchInfo)]),
     ("picasso_batch_destroy", C.c_int, [C.c_void_p]),
 ]

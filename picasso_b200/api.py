@@ -263,9 +263,10 @@ def _check_grid_extent(t, mesh_desc):
 
 
 class Exec:
-    """Execution context: stream, optional skipped-particle counter, bins."""
+    """Execution context: stream, optional skipped-particle counter, bins,
+    optional fixed-point overflow counter (int32 CUDA tensors)."""
 
-    def __init__(self, stream=None, error_count=None, bins=None):
+    def __init__(self, stream=None, error_count=None, bins=None, overflow_count=None):
         self.desc = _abi.Exec()
         s = stream if stream is not None else torch.cuda.current_stream()
         self.desc.stream = s.cuda_stream if hasattr(s, "cuda_stream") else s
@@ -273,10 +274,13 @@ class Exec:
         self.desc.error_count = error_count.data_ptr() if error_count is not None else None
         self._bins = bins
         self.desc.bins = C.pointer(bins.desc) if bins is not None else None
+        self._ovf = overflow_count
+        self.desc.overflow_count = (overflow_count.data_ptr() if overflow_count is not None
+                                    else None)
 
 
-def _exec(stream, error_count, bins):
-    return Exec(stream, error_count, bins)
+def _exec(stream, error_count, bins, overflow_count=None):
+    return Exec(stream, error_count, bins, overflow_count)
 
 
 def _lib():
@@ -292,13 +296,16 @@ class APIC:
     """Picasso::APIC transfers over all particles of the spline."""
 
     @staticmethod
-    def p2g(m_p, c_p, m_i, mu_i, sd, stream=None, error_count=None, bins=None):
+    def p2g(m_p, c_p, m_i, mu_i, sd, stream=None, error_count=None, bins=None,
+            overflow_count=None):
         """APIC::p2g(m_p, c_p, m_i, mu_i, sd): adds mass and momentum into the
-        grid (zero them first for the GridOperator semantics)."""
+        grid (zero them first for the GridOperator semantics).
+        `overflow_count` (int32 CUDA tensor): fixed-point grids add the
+        number of contributions out of the 64-bit range to it."""
         ncomp = c_p.shape[2]
         _check_grid_extent(m_i, sd.desc.mesh)
         _check_grid_extent(mu_i, sd.desc.mesh)
-        ex = _exec(stream, error_count, bins)
+        ex = _exec(stream, error_count, bins, overflow_count)
         check(_lib().picasso_apic_p2g(C.byref(sd.desc), sd.num_particles, ncomp,
                                       particle_field(sd.x), particle_field(m_p),
                                       particle_field(c_p), grid_field(m_i), grid_field(mu_i),
@@ -348,14 +355,15 @@ class PolyPIC:
     """Picasso::PolyPIC transfers (linear 8 modes; quadratic 27 modes)."""
 
     @staticmethod
-    def p2g(m_p, u_p, c_p, mu_i, m_i, dt, sd, stream=None, error_count=None, bins=None):
+    def p2g(m_p, u_p, c_p, mu_i, m_i, dt, sd, stream=None, error_count=None, bins=None,
+            overflow_count=None):
         """PolyPIC::p2g(m_p, u_p, c_p, mu_i, m_i, dt, sd) -- field before mass.
         With bins (cell-sorted particles) the FP32 form runs the tiled kernel
         (bit-identical grid)."""
         ncomp = c_p.shape[2]
         _check_grid_extent(m_i, sd.desc.mesh)
         _check_grid_extent(mu_i, sd.desc.mesh)
-        ex = _exec(stream, error_count, bins)
+        ex = _exec(stream, error_count, bins, overflow_count)
         check(_lib().picasso_polypic_p2g(C.byref(sd.desc), sd.num_particles, ncomp,
                                          particle_field(sd.x), particle_field(m_p),
                                          particle_field(u_p), particle_field(c_p),
@@ -387,9 +395,11 @@ def grid_fill(mesh_desc, f, value=0.0, ncomp=None, stream=None):
                                    C.byref(ex.desc)), "grid_fill")
 
 
-def grid_velocity(mesh_desc, m_i, mu_i, u_i, mass_threshold=1e-12, u64_i=None, stream=None):
-    """u_i = mu_i / m_i (FP64 arithmetic) where m_i > threshold, else 0."""
-    ex = _exec(stream, None, None)
+def grid_velocity(mesh_desc, m_i, mu_i, u_i, mass_threshold=1e-12, u64_i=None, stream=None,
+                  overflow_count=None):
+    """u_i = mu_i / m_i (FP64 arithmetic) where m_i > threshold, else 0.
+    `overflow_count`: fixed-point masses that wrapped negative are counted."""
+    ex = _exec(stream, None, None, overflow_count)
     g64 = grid_field(u64_i) if u64_i is not None else _abi.GridField()
     check(_lib().picasso_grid_velocity(C.byref(mesh_desc), _ncomp_of_grid(mu_i), grid_field(m_i),
                                        grid_field(mu_i), float(mass_threshold), grid_field(u_i),
@@ -397,7 +407,8 @@ def grid_velocity(mesh_desc, m_i, mu_i, u_i, mass_threshold=1e-12, u64_i=None, s
 
 
 def grid_update(mesh_desc, m_i, mu_i, u_i, dt, gravity=(0.0, 0.0, 0.0), f_i=None,
-                mass_threshold=1e-12, walls=None, wall_width=1, u64_i=None, stream=None):
+                mass_threshold=1e-12, walls=None, wall_width=1, u64_i=None, stream=None,
+                overflow_count=None):
     """u_i = (mu_i + dt f_i) / m_i + dt g where m_i > threshold (else 0), then
     wall conditions along non-periodic dimensions: ``walls[d] = (low, high)``
     with "none", "no_slip" or "free_slip"."""
@@ -411,7 +422,7 @@ def grid_update(mesh_desc, m_i, mu_i, u_i, dt, gravity=(0.0, 0.0, 0.0), f_i=None
             prm.wall[d][side] = kinds[walls[d][side]] if walls else _abi.WALL_NONE
     prm.mass_threshold = float(mass_threshold)
     prm.wall_width = int(wall_width)
-    ex = _exec(stream, None, None)
+    ex = _exec(stream, None, None, overflow_count)
     none = _abi.GridField()
     check(_lib().picasso_grid_update(C.byref(mesh_desc), grid_field(m_i), grid_field(mu_i),
                                      grid_field(f_i) if f_i is not None else none,
@@ -446,33 +457,66 @@ class Bins:
         return self.desc.num_tiles[0] * self.desc.num_tiles[1] * self.desc.num_tiles[2]
 
 
+def num_tiles(sd, tile):
+    """Tiles of the spline's mesh for a tile shape (bins per tile)."""
+    nt = 1
+    m = sd.desc.mesh
+    for d in range(3):
+        nb = m.own_extent[d] if m.periodic[d] else m.extent[d]
+        nt *= -(-nb // tile[d])
+    return nt
+
+
+class SortBuffers:
+    """Outputs of cell_sort kept across the steps of a time loop (key,
+    perm, tile offsets, tile work items and the workspace), so that its
+    sorts allocate nothing."""
+
+    def __init__(self, sd, tile=(4, 8, 8)):
+        dev = sd.x.device
+        n = max(sd.num_particles, 1)
+        nt = num_tiles(sd, tile)
+        self.tile = tuple(tile)
+        self.key = torch.empty(n, dtype=torch.int32, device=dev)
+        self.perm = torch.empty(n, dtype=torch.int32, device=dev)
+        self.tile_offset = torch.empty(nt + 1, dtype=torch.int64, device=dev)
+        self.tile_items = torch.empty(nt + 1, dtype=torch.int32, device=dev)
+        self.workspace = sort_workspace(sd, tile)
+
+
 def cell_sort(sd, tile=(4, 8, 8), chunk=4096, stream=None, workspace=None, p2g_lanes=0,
-              keys=None):
+              keys=None, out=None):
     """Stable sort of the spline's particles by (tile, bin).  Returns
     (key, perm, bins): keys and permutation as int32 tensors holding uint32
     values, and the Bins to pass to the transfers once the particle members
     have been permuted (see permute / permute_members).  `p2g_lanes` (1, 2, 4;
     0 = library choice) is the tiled P2G's lanes per particle.  `keys`: the
     particles' keys for this tile shape as APIC.g2p_advect(key_tile=tile)
-    returned them; the sort then starts from them instead of the positions."""
+    returned them; the sort then starts from them instead of the positions.
+    `out`: a SortBuffers for this spline and tile shape whose tensors receive
+    the results (nothing is allocated); the returned Bins then point into
+    them, so they stay valid until the next sort into the same buffers."""
     lib = _lib()
     n = sd.num_particles
     t3 = (C.c_int32 * 3)(*tile)
-    nbytes = C.c_int64()
-    check(lib.picasso_cell_sort_workspace(C.byref(sd.desc), n, t3, C.byref(nbytes)),
-          "cell_sort_workspace")
     dev = sd.x.device
-    if workspace is None or workspace.numel() < nbytes.value:
-        workspace = torch.empty(max(nbytes.value, 1), dtype=torch.uint8, device=dev)
-    key = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
-    perm = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
-    nt = 1
-    for d in range(3):
-        m = sd.desc.mesh
-        nb = m.own_extent[d] if m.periodic[d] else m.extent[d]
-        nt *= -(-nb // tile[d])
-    tile_offset = torch.empty(nt + 1, dtype=torch.int64, device=dev)
-    tile_items = torch.empty(nt + 1, dtype=torch.int32, device=dev)
+    nt = num_tiles(sd, tile)
+    if out is not None:
+        if (out.tile != tuple(tile) or out.key.numel() < n or out.perm.numel() < n
+                or out.tile_offset.numel() != nt + 1):
+            raise ValueError("SortBuffers made for another particle count or tile shape")
+        key, perm, tile_offset, tile_items = out.key, out.perm, out.tile_offset, out.tile_items
+        workspace = out.workspace
+    else:
+        nbytes = C.c_int64()
+        check(lib.picasso_cell_sort_workspace(C.byref(sd.desc), n, t3, C.byref(nbytes)),
+              "cell_sort_workspace")
+        if workspace is None or workspace.numel() < nbytes.value:
+            workspace = torch.empty(max(nbytes.value, 1), dtype=torch.uint8, device=dev)
+        key = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
+        perm = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
+        tile_offset = torch.empty(nt + 1, dtype=torch.int64, device=dev)
+        tile_items = torch.empty(nt + 1, dtype=torch.int32, device=dev)
     bins = _abi.Bins()
     ex = _exec(stream, None, None)
     if keys is not None:
@@ -623,6 +667,15 @@ class Batch:
     def status(self, stream=None):
         """Synchronises the stream; raises if a dependency wait ran out."""
         check(_lib().picasso_batch_status(self._h, self._stream(stream)), "batch_status")
+
+    def set_wait_limit(self, polls):
+        """Bound of the fused step's dependency waits (polls of ~0.25 us)."""
+        check(_lib().picasso_batch_set_wait_limit(self._h, int(polls)), "batch_set_wait_limit")
+
+    def cancel(self, stream=None):
+        """Makes every dependency wait of the following fused steps give up
+        until status() has reported it."""
+        check(_lib().picasso_batch_cancel(self._h, self._stream(stream)), "batch_cancel")
 
     def info(self):
         inf = _abi.BatchInfo()

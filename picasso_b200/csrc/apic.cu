@@ -162,6 +162,7 @@ extern "C" picasso_status picasso_apic_p2g(const picasso_spline* sd, int64_t num
     int* err = exec ? exec->error_count : nullptr;
     PField x = make_pfield(x_p), m = make_pfield(m_p), c = make_pfield(c_p);
     GField gm = make_gfield(m_i), gmu = make_gfield(mu_i);
+    gm.overflow = gmu.overflow = exec ? exec->overflow_count : nullptr;
     if (exec && exec->bins) {
         // bins describe particles sorted for this spline
         if (exec->bins->order != sd->order || exec->bins->location != sd->location)

@@ -50,7 +50,7 @@ __host__ __device__ constexpr int p2g_variant(bool f32, int order, int lpp)
                : order - 1;
 }
 constexpr int kNodeItem = 4096;           // nodes per fill / velocity item
-constexpr unsigned kWaitPolls = 1u << 22;  // ~1-2 s of polling before a wait gives up
+constexpr unsigned kWaitPolls = 1u << 22;  // default bound: ~1-2 s of polling
 
 struct BInst {
     P2GArgs p2g;  // tiled P2G arguments (precision form)
@@ -71,7 +71,8 @@ struct BatchDev {
     uint32_t* done;          // kPhases * count completion counters
     uint32_t* head;          // queue heads: one per phase launch, then one per P2G
                              // variant launch (fused mode uses head[0])
-    int* status;             // bit 0: a dependency wait ran out
+    int* status;             // bit 0: a dependency wait ran out; bit 1: cancelled
+    unsigned wait_polls;     // polls before a dependency wait gives up
     int count;
 };
 
@@ -90,7 +91,7 @@ __device__ bool wait_for(const BatchDev& B, const uint32_t* counter, uint32_t ta
     if (lane == 0) {
         unsigned polls = 0;
         while (ld_acquire(counter) < target) {
-            if (*(volatile int*)B.status != 0 || ++polls > kWaitPolls) {
+            if (*(volatile int*)B.status != 0 || ++polls > B.wait_polls) {
                 atomicOr(B.status, 1);
                 ok = 0;
                 break;
@@ -640,6 +641,7 @@ extern "C" picasso_status picasso_batch_create(const picasso_batch_instance* ins
     b->dev.done = reinterpret_cast<uint32_t*>(base + o_done);
     b->dev.head = b->dev.done + (size_t)kPhases * count;
     b->dev.status = reinterpret_cast<int*>(base + o_status);
+    b->dev.wait_polls = kWaitPolls;
     b->dev.count = count;
     picasso_status st = f32 ? configure<true>(b) : configure<false>(b);
     if (st) {
@@ -708,6 +710,30 @@ extern "C" picasso_status picasso_batch_status(picasso_batch* b, void* stream)
         PB_CUDA_TRY(cudaMemset(b->dev.status, 0, sizeof(int)));
         return PICASSO_ERR_TIMEOUT;
     }
+    return PICASSO_OK;
+}
+
+extern "C" picasso_status picasso_batch_set_wait_limit(picasso_batch* b, uint32_t polls)
+{
+    if (!b) return PICASSO_ERR_INVALID_ARGUMENT;
+    b->dev.wait_polls = polls;
+    if (b->graph) {  // the captured launches hold the old limit
+        int prev = 0;
+        PB_CUDA_TRY(cudaGetDevice(&prev));
+        PB_CUDA_TRY(cudaSetDevice(b->device));
+        const cudaError_t e = cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+        cudaSetDevice(prev);
+        PB_CUDA_TRY(e);
+    }
+    return PICASSO_OK;
+}
+
+extern "C" picasso_status picasso_batch_cancel(picasso_batch* b, void* stream)
+{
+    if (!b) return PICASSO_ERR_INVALID_ARGUMENT;
+    // one byte of the status word: bit 1 (cancelled); bit 0 keeps its meaning
+    PB_CUDA_TRY(cudaMemsetAsync(b->dev.status, 2, 1, static_cast<cudaStream_t>(stream)));
     return PICASSO_OK;
 }
 

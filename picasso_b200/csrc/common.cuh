@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "../../include/picasso_b200.h"
 
 namespace pb {
@@ -88,6 +90,7 @@ struct GField {
     char* data;
     int64_t s[4];
     int32_t fixed_bits;
+    int32_t* overflow;  // optional counter of fixed-point values out of range
 
     __device__ __forceinline__ int64_t index(int i, int j, int k, int c) const
     {
@@ -106,7 +109,26 @@ inline GField make_gfield(const picasso_grid_field& f)
     g.data = static_cast<char*>(f.data);
     for (int d = 0; d < 4; ++d) g.s[d] = f.stride[d];
     g.fixed_bits = f.fixed_bits;
+    g.overflow = nullptr;
     return g;
+}
+
+// Fixed-point headroom: a value whose magnitude times 2^fixed_bits reaches
+// 2^62 leaves no room for the sums it enters (a 64-bit sum wraps at 2^63).
+constexpr float kFixedLimitF = 4.611686018427387904e18f;  // 2^62
+constexpr double kFixedLimitD = 4.611686018427387904e18;
+
+// Rounds a scaled value to fixed point; counts it in g.overflow (when given)
+// if it is out of range (the conversion saturates, so the sum is wrong).
+__device__ __forceinline__ long long to_fixed(const GField& g, float scaled)
+{
+    if (!(fabsf(scaled) < kFixedLimitF) && g.overflow) atomicAdd(g.overflow, 1);
+    return __float2ll_rn(scaled);
+}
+__device__ __forceinline__ long long to_fixed(const GField& g, double scaled)
+{
+    if (!(fabs(scaled) < kFixedLimitD) && g.overflow) atomicAdd(g.overflow, 1);
+    return __double2ll_rn(scaled);
 }
 
 // ---------------------------------------------------------------------------
@@ -315,14 +337,14 @@ struct AccFixed {
     __device__ __forceinline__ static void add(const GField& g, int i, int j, int k, int c,
                                                double v, double scale)
     {
-        long long q = __double2ll_rn(v * scale);
+        long long q = to_fixed(g, v * scale);
         atomicAdd(reinterpret_cast<unsigned long long*>(g.ptr<long long>(i, j, k, c)),
                   (unsigned long long)q);
     }
     __device__ __forceinline__ static void add(const GField& g, int i, int j, int k, int c,
                                                float v, float scale)
     {
-        long long q = __float2ll_rn(v * scale);
+        long long q = to_fixed(g, v * scale);
         atomicAdd(reinterpret_cast<unsigned long long*>(g.ptr<long long>(i, j, k, c)),
                   (unsigned long long)q);
     }

@@ -167,6 +167,7 @@ extern "C" picasso_status picasso_grid_velocity(const picasso_mesh* mesh, int32_
     Box b = owned_box(*mesh);
     GField gm = make_gfield(m_i), gmu = make_gfield(mu_i), gu = make_gfield(u_i);
     GField gu64 = make_gfield(u64_i);
+    gm.overflow = exec ? exec->overflow_count : nullptr;
     cudaStream_t s = stream_of(exec);
     const bool fixed = m_i.dtype == PICASSO_I64_FIXED;
     const double inv_m = fixed ? ldexp(1.0, -m_i.fixed_bits) : 1.0;
@@ -227,6 +228,7 @@ extern "C" picasso_status picasso_grid_update(const picasso_mesh* mesh, picasso_
     Box b = owned_box(*mesh);
     GField gm = make_gfield(m_i), gmu = make_gfield(mu_i), gf = make_gfield(f_i);
     GField gu = make_gfield(u_i), gu64 = make_gfield(u64_i);
+    gm.overflow = exec ? exec->overflow_count : nullptr;
     cudaStream_t s = stream_of(exec);
     const unsigned blocks = grid_for(b.count(), 256, 148LL * 32);
     const bool f64f = !force || f_i.dtype == PICASSO_F64;

@@ -43,6 +43,16 @@ inline Box owned_box(const picasso_mesh& m)
     return b;
 }
 
+// A fixed-point node mass is a sum of non-negative contributions: a negative
+// sum has wrapped past 2^63 (too many fraction bits for the mass at that
+// node).  Counted in gm.overflow when the caller asked for it.
+template <class MT>
+__device__ __forceinline__ void count_wrapped_mass(const GField& gm, MT raw)
+{
+    if constexpr (std::is_same<MT, long long>::value)
+        if (raw < 0 && gm.overflow) atomicAdd(gm.overflow, 1);
+}
+
 // u = mu / m where m > threshold else 0; all arithmetic in FP64.  CG loads
 // the accumulators through L2 only (grids written earlier in the same launch).
 template <class MT, class UT, int NC, bool CG = false>
@@ -51,7 +61,9 @@ __device__ __forceinline__ void velocity_node(const GField& gm, const GField& gm
                                               int k, double thr, double inv_m, double inv_mu)
 {
     auto load = [](const MT* a) { return CG ? __ldcg(a) : *a; };
-    const double m = (double)load(gm.ptr<MT>(i, j, k, 0)) * inv_m;
+    const MT raw = load(gm.ptr<MT>(i, j, k, 0));
+    count_wrapped_mass(gm, raw);
+    const double m = (double)raw * inv_m;
     const bool keep = m > thr;
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
@@ -76,7 +88,9 @@ __device__ __forceinline__ void update_node(const GridUpdate& P, const GField& g
                                             const GField& gmu, const GField& gf, const GField& gu,
                                             const GField& gu64, int i, int j, int k)
 {
-    const double m = __dmul_rn((double)*gm.ptr<MT>(i, j, k, 0), P.inv_m);
+    const MT raw = *gm.ptr<MT>(i, j, k, 0);
+    count_wrapped_mass(gm, raw);
+    const double m = __dmul_rn((double)raw, P.inv_m);
     const bool keep = m > P.thr;
     double u[3];
 #pragma unroll

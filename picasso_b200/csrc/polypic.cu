@@ -472,7 +472,7 @@ polypic_p2g_tiled_kernel(MeshP mp, TileP tp, int64_t n, PField x, PField m, PFie
         polypic_p2g_particle<ORDER, NC, false, float, float>(
             mp, p, x, m, u, dt, -1, err, place,
             [&](int f, int i, int j, int k, float v) {
-                const long long q = __float2ll_rn(v * (f == 0 ? scale_m : scale_mu));
+                const long long q = to_fixed(f == 0 ? gm : gmu, v * (f == 0 ? scale_m : scale_mu));
                 const int e = f * nodes + (i * tp.NT[1] + j) * tp.NT[2] + k;
                 atomicAdd(&pp_tacc[e], (unsigned int)(q & 0xFFFF));
                 atomicAdd(&pp_tacc[slice + e], (unsigned int)((q >> 16) & 0xFFFF));
@@ -735,6 +735,7 @@ extern "C" picasso_status picasso_polypic_p2g(const picasso_spline* sd, int64_t 
     int* err = exec ? exec->error_count : nullptr;
     PField x = make_pfield(x_p), m = make_pfield(m_p), u = make_pfield(u_p), c = make_pfield(c_p);
     GField gmu = make_gfield(mu_i), gm = make_gfield(m_i);
+    gmu.overflow = gm.overflow = exec ? exec->overflow_count : nullptr;
     bool tiled = false;
     TileP tp;
     // (the tile's 32-bit slice sums are exact for work items of at most

@@ -10,7 +10,6 @@
 // original order (warp __match_any_sync + a per-warp running count, then a
 // prefix over the block's warps), so every pass is stable.
 #include <cmath>
-#include <mutex>
 
 #include "binkey.cuh"
 
@@ -527,23 +526,17 @@ namespace pb {
 constexpr int64_t kStaticSortScratchBytes = 32LL << 20;  // 32 MiB
 static __device__ __align__(256) unsigned char g_sort_scratch[kStaticSortScratchBytes];
 
-// Device address of g_sort_scratch on the current device, looked up once per
-// device (the host-side name of a __device__ array is not a device address).
+// Device address of g_sort_scratch in the current context.  It is looked up
+// on every call: the host-side name of a __device__ array is not a device
+// address, and a cached address would go stale when the application resets
+// the device or its primary context (the module is then loaded again and the
+// array may move).  The lookup costs microseconds, small next to the sort's
+// launches.
 static picasso_status static_sort_scratch(void** out)
 {
-    constexpr int kMaxDevices = 64;
-    static std::mutex mu;
-    static void* addr[kMaxDevices] = {};
-    int dev = 0;
-    PB_CUDA_TRY(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kMaxDevices) return PICASSO_ERR_NO_DEVICE;
-    std::lock_guard<std::mutex> lock(mu);
-    if (!addr[dev]) {
-        void* p = nullptr;
-        PB_CUDA_TRY(cudaGetSymbolAddress(&p, g_sort_scratch));
-        addr[dev] = p;
-    }
-    *out = addr[dev];
+    void* p = nullptr;
+    PB_CUDA_TRY(cudaGetSymbolAddress(&p, g_sort_scratch));
+    *out = p;
     return PICASSO_OK;
 }
 

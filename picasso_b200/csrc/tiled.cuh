@@ -662,7 +662,8 @@ __device__ void p2g_item(const P2GArgs& A, int64_t t, int64_t a, int64_t b, floa
             for (int f = 0; f < 4; ++f) {
                 const float v = tile[f * tp.P + idx];
                 if (v != 0.f) {
-                    const long long q = __float2ll_rn(v * (f == 0 ? A.scale_m : A.scale_mu));
+                    const long long q =
+                        to_fixed(f == 0 ? A.gm : A.gmu, v * (f == 0 ? A.scale_m : A.scale_mu));
                     unsigned long long* dst = reinterpret_cast<unsigned long long*>(
                         f == 0 ? A.gm.ptr<long long>(gi, gj, gk, 0)
                                : A.gmu.ptr<long long>(gi, gj, gk, f - 1));

@@ -60,3 +60,22 @@ def rel_err(a, b):
     b = np.asarray(b, dtype=np.float64)
     den = np.max(np.abs(b))
     return float(np.max(np.abs(a - b)) / (den if den > 0 else 1.0))
+
+
+def node_rel_err(a, b, mask=None):
+    """Largest per-entry relative error: for every entry (grid node or
+    particle, leading axes) the max-norm of a - b over its components divided
+    by the max-norm of b, over the entries selected by `mask` (e.g. nodes
+    with mass above the velocity threshold) whose b is not zero."""
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    if a.ndim == b.ndim and mask is not None and a.ndim > np.asarray(mask).ndim:
+        axes = tuple(range(np.asarray(mask).ndim, a.ndim))
+    else:
+        axes = tuple(range(1, a.ndim)) if mask is None else ()
+    num = np.max(np.abs(a - b), axis=axes) if axes else np.abs(a - b)
+    den = np.max(np.abs(b), axis=axes) if axes else np.abs(b)
+    sel = den > 0
+    if mask is not None:
+        sel &= np.asarray(mask, dtype=bool)
+    return float(np.max(num[sel] / den[sel])) if np.any(sel) else 0.0

@@ -8,7 +8,10 @@ persistent launches fed by one work queue.  Checked here:
     arithmetic on the same particles), over two consecutive steps;
   * every instance against the FP64 oracle (normwise relative <= 1e-5 in the
     precision form, <= 1e-12 in the FP64 form);
-  * FP64 form against its sequential calls (atomic order only: <= 1e-12).
+  * FP64 form against its sequential calls (atomic order only: <= 1e-12);
+  * the bounded dependency waits of the fused launch: a wait limit of 0
+    polls and a host-side cancel make waits give up, the launch ends and
+    the batch status reports it.
 """
 
 import numpy as np
@@ -17,8 +20,8 @@ import torch
 
 import oracle
 from particles import clustered_particles, periodic_mesh, rel_err, uniform_particles
-from picasso_b200 import (Batch, BatchInstance, FieldLocation, FixedGrid, cell_sort,
-                          create_spline, permute_members)
+from picasso_b200 import (Batch, BatchInstance, FieldLocation, FixedGrid, PicassoError, _abi,
+                          cell_sort, create_spline, permute_members)
 
 pytestmark = pytest.mark.gpu
 BITS = 36
@@ -156,5 +159,65 @@ def test_fp64_batch_matches_sequential(cuda, hosts):
         assert rel_err(a1.cpu().numpy(), a0.cpu().numpy()) <= 1e-12
         assert rel_err(u1.cpu().numpy(), u0.cpu().numpy()) <= 1e-12
         assert rel_err(c1.cpu().numpy(), c0.cpu().numpy()) <= 1e-12
+    ref.close()
+    bat.close()
+
+
+def _expect_timeout(bat):
+    with pytest.raises(PicassoError) as e:
+        bat.status()
+    assert e.value.status == _abi.ERR_TIMEOUT
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_wait_that_runs_out_ends_the_launch(cuda, hosts, graph):
+    """A fused step whose dependency waits may poll 0 times: the items that
+    find their instance's previous phase unfinished give up at once, the
+    launch still ends, and status() reports PICASSO_ERR_TIMEOUT (the bounded
+    device wait, run out on purpose; nothing faults or hangs).  Restoring
+    the default limit gives complete steps again."""
+    runs = _build(True, hosts)
+    bat = Batch([r["inst"] for r in runs], mode="fused")
+    # the first wave of persistent warps takes fill and P2G items together, so
+    # the P2G items poll while their instance's fill is still running
+    bat.set_wait_limit(0)
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    bat.step(graph=graph)
+    t1.record()
+    torch.cuda.synchronize()
+    assert t0.elapsed_time(t1) < 1000.0  # ms: the launch did not wait out a long bound
+    _expect_timeout(bat)
+    bat.set_wait_limit(1 << 22)
+    bat.step(graph=graph)
+    bat.status()  # complete again
+    bat.close()
+
+
+def test_cancel_ends_fused_steps_until_reported(cuda, hosts):
+    """picasso_batch_cancel: every wait of the next fused steps gives up at
+    once until status() has reported PICASSO_ERR_TIMEOUT; after that the
+    batch steps normally and matches the sequential calls from the same
+    particles."""
+    runs = _build(True, hosts)
+    bat = Batch([r["inst"] for r in runs], mode="fused")
+    saved = [r["c"].clone() for r in runs]
+    bat.cancel()
+    bat.step(graph=False)
+    bat.step(graph=True)
+    _expect_timeout(bat)
+    # restart from the saved particle state; the step is complete again
+    for r, c0 in zip(runs, saved):
+        r["c"].copy_(c0)
+    ref_runs = _build(True, hosts)
+    ref = Batch([r["inst"] for r in ref_runs], mode="fused")
+    ref.step_sequential()
+    bat.step(graph=True)
+    bat.status()
+    for (a0, u0, c0), (a1, u1, c1) in zip(_state(ref_runs), _state(runs)):
+        assert torch.equal(a0, a1)
+        assert torch.equal(u0, u1)
+        assert torch.equal(c0, c1)
     ref.close()
     bat.close()
