@@ -152,6 +152,15 @@ typedef struct picasso_bins {
     const uint32_t* tile_items;  /* device, num_tiles_total + 1: first work item
                                     of each tile (exclusive prefix of
                                     ceil(count / chunk)) */
+    const void* records;         /* optional device, 16-byte aligned: the spline
+                                    record of every (sorted) particle as
+                                    picasso_spline_records writes it for these
+                                    bins; the tiled P2G and G2P (not the one
+                                    with advection) then read it instead of the
+                                    positions.  Set by the caller after the
+                                    permutation; the sort sets it to NULL.  It
+                                    must be rewritten whenever a position
+                                    changes. */
 } picasso_bins;
 
 /* Execution context of one call. */
@@ -367,6 +376,22 @@ PICASSO_API picasso_status picasso_cell_sort_keys(const picasso_spline* sd, int6
                                                   int64_t* tile_offset, uint32_t* tile_items,
                                                   void* workspace, int64_t workspace_bytes,
                                                   picasso_bins* bins_out,
+                                                  const picasso_exec* exec);
+
+/* Spline records of sorted particles for the tiled transfers: records[p]
+ * (16 bytes, device, 16-byte aligned) = the in-cell fractions (t_x, t_y, t_z)
+ * of particle p's logical position as FP32 and, in the fourth word, its sort
+ * key (uint32) for `bins`.  Both are formed from the FP64 position with the
+ * arithmetic every kernel uses, so P2G / G2P that read the records (set
+ * bins->records) build the same splines and bins as from the positions, while
+ * reading 16 instead of 24 bytes per particle and no FP64 arithmetic.  Call it
+ * after picasso_permute (x_p in sorted order) and after every position
+ * change.  No counterpart in the reference (its splines are evaluated from
+ * the positions in every transfer, ParticleInterpolation.hpp:88-105). */
+PICASSO_API picasso_status picasso_spline_records(const picasso_spline* sd,
+                                                  int64_t num_particles,
+                                                  picasso_particle_field x_p,
+                                                  const picasso_bins* bins, void* records,
                                                   const picasso_exec* exec);
 
 /* picasso_cell_sort for callers that cannot allocate device memory when they

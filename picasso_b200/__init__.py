@@ -34,6 +34,7 @@ from .api import (  # noqa: F401
     permute,
     permute_members,
     sort_workspace,
+    spline_records,
     tune_tiled_step,
 )
 

@@ -58,7 +58,7 @@ class Bins(C.Structure):
     _fields_ = [("tile", C.c_int32 * 3), ("num_tiles", C.c_int32 * 3),
                 ("bin_extent", C.c_int32 * 3), ("order", C.c_int32), ("location", C.c_int32),
                 ("chunk", C.c_int32), ("p2g_lanes", C.c_int32), ("tile_offset", C.c_void_p),
-                ("tile_items", C.c_void_p)]
+                ("tile_items", C.c_void_p), ("records", C.c_void_p)]
 
 
 class Exec(C.Structure):
@@ -147,6 +147,9 @@ SIGNATURES = [
      [C.c_int64, C.c_int32, C.c_void_p, ParticleField, ParticleField, C.POINTER(Exec)]),
     ("picasso_mat3_inverse", C.c_int,
      [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+      C.POINTER(Exec)]),
+    ("picasso_spline_records", C.c_int,
+     [C.POINTER(Spline), C.c_int64, ParticleField, C.POINTER(Bins), C.c_void_p,
       C.POINTER(Exec)]),
     ("picasso_batch_create", C.c_int,
      [C.POINTER(BatchInstance), C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]),

@@ -445,12 +445,21 @@ def advect(mesh_desc, x_p, c_p, dt, stream=None):
 
 
 class Bins:
-    """Result of cell_sort: the C descriptor plus the tensors it points to."""
+    """Result of cell_sort: the C descriptor plus the tensors it points to
+    (and the spline records attached with spline_records, if any)."""
 
     def __init__(self, desc, tile_offset, tile_items):
         self.desc = desc
         self.tile_offset = tile_offset
         self.tile_items = tile_items
+        self.records = None
+
+    def attach_records(self, records):
+        """Let the tiled transfers read these spline records (an (N, 4)
+        float32 CUDA tensor from spline_records) instead of the positions;
+        None detaches them."""
+        self.records = records
+        self.desc.records = records.data_ptr() if records is not None else None
 
     @property
     def num_tiles(self):
@@ -535,6 +544,27 @@ def cell_sort(sd, tile=(4, 8, 8), chunk=4096, stream=None, workspace=None, p2g_l
               "cell_sort")
     bins.p2g_lanes = int(p2g_lanes)
     return key[:n], perm[:n], Bins(bins, tile_offset, tile_items)
+
+
+def spline_records(sd, bins, out=None, attach=True, stream=None):
+    """picasso_spline_records: the (N, 4) float32 tensor of the sorted
+    particles' spline records (in-cell fractions and sort key) for `bins`;
+    with attach=True the bins then carry them, so that the tiled P2G / G2P
+    read them instead of the positions.  Call again after the positions
+    change."""
+    n = sd.num_particles
+    if out is None:
+        out = torch.empty((max(n, 1), 4), dtype=torch.float32, device=sd.x.device)
+    elif (out.dtype != torch.float32 or out.shape[0] < n or out.shape[1:] != (4,)
+          or not out.is_contiguous()):
+        raise ValueError("out: contiguous (N, 4) float32 tensor")
+    ex = _exec(stream, None, None)
+    check(_lib().picasso_spline_records(C.byref(sd.desc), n, particle_field(sd.x),
+                                        C.byref(bins.desc), out.data_ptr(), C.byref(ex.desc)),
+          "spline_records")
+    if attach:
+        bins.attach_records(out)
+    return out
 
 
 def sort_workspace(sd, tile=(4, 8, 8)):

@@ -18,22 +18,19 @@ struct BinP {  // bins of one mesh / spline / tile shape
     uint32_t nkeys;  // valid keys are < nkeys; out-of-mesh particles get nkeys
 };
 
-__device__ __forceinline__ uint32_t particle_key(const BinP& bp, const double xs[3])
+// Key of a particle from the (unwrapped) stencil starts s[d] of its spline.
+__device__ __forceinline__ uint32_t key_from_starts(const BinP& bp, const int s[3])
 {
     const int K = bp.order + 1;
-    const int first = (bp.order == 1) ? 0 : -1;
-    const double shift = (bp.order == 2) ? 0.5 : 0.0;
     int q[3], r[3];  // tile index and bin inside the tile
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-        const double x0 = logical_coord(xs[d], bp.mp.lo[d], bp.mp.rdx[d], shift);
-        const int s = (int)floor(x0) + first;
         int b;
         if (bp.mp.periodic[d]) {
             // (s - own_lo) mod nb; one period covers every particle inside or
             // next to the owned box, the remainder the rest
             const int nb = bp.nb[d];
-            b = s - bp.mp.own_lo[d];
+            b = s[d] - bp.mp.own_lo[d];
             if (b < 0) b += nb;
             else if (b >= nb) b -= nb;
             if ((unsigned)b >= (unsigned)nb) {
@@ -41,8 +38,8 @@ __device__ __forceinline__ uint32_t particle_key(const BinP& bp, const double xs
                 if (b < 0) b += nb;
             }
         } else {
-            if (s < 0 || s > bp.mp.ext[d] - K) return bp.nkeys;
-            b = s;
+            if (s[d] < 0 || s[d] > bp.mp.ext[d] - K) return bp.nkeys;
+            b = s[d];
         }
         if (bp.tshift[d] >= 0) {
             q[d] = b >> bp.tshift[d];
@@ -55,6 +52,19 @@ __device__ __forceinline__ uint32_t particle_key(const BinP& bp, const double xs
     const uint32_t tl = ((uint32_t)q[0] * bp.nt[1] + (uint32_t)q[1]) * bp.nt[2] + (uint32_t)q[2];
     const uint32_t ll = ((uint32_t)r[0] * bp.tile[1] + (uint32_t)r[1]) * bp.tile[2] + (uint32_t)r[2];
     return tl * bp.tsize + ll;
+}
+
+__device__ __forceinline__ uint32_t particle_key(const BinP& bp, const double xs[3])
+{
+    const int first = (bp.order == 1) ? 0 : -1;
+    const double shift = (bp.order == 2) ? 0.5 : 0.0;
+    int s[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const double x0 = logical_coord(xs[d], bp.mp.lo[d], bp.mp.rdx[d], shift);
+        s[d] = (int)floor(x0) + first;
+    }
+    return key_from_starts(bp, s);
 }
 
 // BinP of a spline (mesh, order, location) and tile shape; *ntiles = the

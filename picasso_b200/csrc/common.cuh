@@ -252,20 +252,11 @@ __device__ __forceinline__ void spline_eval_f64(double x, double lo, double dx, 
         sp.d[n] = lo + (double)(sp.s0 + n) * dx - x;
 }
 
-// Reduced-precision evaluation: the logical position and its integer part
-// are formed in FP64 from the FP64 position; the in-cell fraction, weights
-// and distances are then formed in R from the fraction, so no large
-// coordinates are cancelled in R.
+// Weights, gradients and distances of one dimension from the in-cell
+// fraction t of the logical position (t = x0 - floor(x0)), in R; h = dx.
 template <int ORDER, class R>
-__device__ __forceinline__ void spline_eval_frac(double x, double lo, double dx, double rdx,
-                                                 Spline1D<ORDER, R>& sp)
+__device__ __forceinline__ void spline_from_frac(R t, R h, double rdx, Spline1D<ORDER, R>& sp)
 {
-    double x0 = logical_coord(x, lo, rdx, SplineTraits<ORDER>::shift);
-    double fl = floor(x0);
-    int s0 = (int)fl;
-    R t = (R)(x0 - fl);
-    R h = (R)dx;
-    sp.s0 = s0 + SplineTraits<ORDER>::first;
     if (ORDER == 1) {
         sp.w[0] = R(1) - t;
         sp.w[1] = t;
@@ -295,6 +286,34 @@ __device__ __forceinline__ void spline_eval_frac(double x, double lo, double dx,
 #pragma unroll
     for (int n = 0; n < SplineTraits<ORDER>::K; ++n)
         sp.d[n] = (R(SplineTraits<ORDER>::first + n + SplineTraits<ORDER>::shift) - t) * h;
+}
+
+// In-cell fraction of the logical position of x and the stencil start, the
+// logical position and its integer part formed in FP64 (step by step, as in
+// every kernel, so the stencil start is bit-identical everywhere).
+template <int ORDER>
+__device__ __forceinline__ float logical_frac(double x, double lo, double rdx, int& s0)
+{
+    const double x0 = logical_coord(x, lo, rdx, SplineTraits<ORDER>::shift);
+    const double fl = floor(x0);
+    s0 = (int)fl + SplineTraits<ORDER>::first;
+    return (float)(x0 - fl);
+}
+
+// Reduced-precision evaluation: the logical position and its integer part
+// are formed in FP64 from the FP64 position; the in-cell fraction, weights
+// and distances are then formed in R from the fraction, so no large
+// coordinates are cancelled in R.
+template <int ORDER, class R>
+__device__ __forceinline__ void spline_eval_frac(double x, double lo, double dx, double rdx,
+                                                 Spline1D<ORDER, R>& sp)
+{
+    double x0 = logical_coord(x, lo, rdx, SplineTraits<ORDER>::shift);
+    double fl = floor(x0);
+    int s0 = (int)fl;
+    R t = (R)(x0 - fl);
+    sp.s0 = s0 + SplineTraits<ORDER>::first;
+    spline_from_frac<ORDER, R>(t, (R)dx, rdx, sp);
 }
 
 // Periodic wrap / bounds check of a stencil start: fills the K resolved

@@ -439,6 +439,7 @@ static picasso_status cell_sort_impl(const picasso_spline* sd, int64_t num_parti
         bins_out->p2g_lanes = 0;
         bins_out->tile_offset = tile_offset;
         bins_out->tile_items = tile_items;
+        bins_out->records = nullptr;
     }
     return PICASSO_OK;
 }
@@ -508,6 +509,61 @@ extern "C" picasso_status picasso_permute(int64_t num_particles, int32_t ncomp,
     else
         permute_kernel<float><<<blocks, 256, 0, s>>>(num_particles, ncomp, perm, make_pfield(src),
                                                      make_pfield(dst));
+    return check_launch();
+}
+
+// ---------------------------------------------------------------------------
+// Spline records
+// ---------------------------------------------------------------------------
+// rec[p] = (t_x, t_y, t_z, key): the in-cell fraction of the particle's
+// logical position along each dimension (FP32, rounded from the FP64
+// position exactly as the transfer kernels round it) and its sort key for
+// the bins' tile shape (the cell sort's key, stencil starts from the same
+// FP64 arithmetic), so a transfer that reads the record builds the same
+// spline and bin as one that reads the position.
+namespace pb {
+
+template <int ORDER>
+__global__ void records_kernel(BinP bp, int64_t n, PField x, float4* rec)
+{
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
+        int s[3];
+        float t[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+            t[d] = logical_frac<ORDER>(x.get<double>(p, d), bp.mp.lo[d], bp.mp.rdx[d], s[d]);
+        rec[p] = make_float4(t[0], t[1], t[2], __uint_as_float(key_from_starts(bp, s)));
+    }
+}
+
+}  // namespace pb
+
+extern "C" picasso_status picasso_spline_records(const picasso_spline* sd, int64_t num_particles,
+                                                 picasso_particle_field x_p,
+                                                 const picasso_bins* bins, void* records,
+                                                 const picasso_exec* exec)
+{
+    if (!sd || !bins || num_particles < 0) return PICASSO_ERR_INVALID_ARGUMENT;
+    if (bins->order != sd->order || bins->location != sd->location)
+        return PICASSO_ERR_INVALID_ARGUMENT;
+    BinP bp;
+    int64_t ntiles = 0;
+    picasso_status st = make_binp(sd, bins->tile, &bp, &ntiles);
+    if (st) return st;
+    for (int d = 0; d < 3; ++d)
+        if (bins->num_tiles[d] != bp.nt[d] || bins->bin_extent[d] != bp.nb[d])
+            return PICASSO_ERR_INVALID_ARGUMENT;
+    if ((st = validate_pfield(num_particles, x_p, PICASSO_F64))) return st;
+    if (num_particles == 0) return PICASSO_OK;
+    if (!records || reinterpret_cast<uintptr_t>(records) % 16) return PICASSO_ERR_INVALID_ARGUMENT;
+    cudaStream_t s = stream_of(exec);
+    const PField x = make_pfield(x_p);
+    float4* rec = static_cast<float4*>(records);
+    const unsigned blocks = grid_for(num_particles, 256);
+    if (sd->order == 1) records_kernel<1><<<blocks, 256, 0, s>>>(bp, num_particles, x, rec);
+    else if (sd->order == 2) records_kernel<2><<<blocks, 256, 0, s>>>(bp, num_particles, x, rec);
+    else records_kernel<3><<<blocks, 256, 0, s>>>(bp, num_particles, x, rec);
     return check_launch();
 }
 

@@ -19,7 +19,7 @@ struct G2PThreads {
     static constexpr int value = ORDER == 3 ? 32 : 64;
 };
 
-template <int ORDER, int LPP>
+template <int ORDER, int LPP, bool REC>
 __global__ void __launch_bounds__(32, (P2GOccupancy<ORDER, LPP>::value))
 p2g_tiled_kernel(P2GArgs A, int64_t n)
 {
@@ -31,10 +31,10 @@ p2g_tiled_kernel(P2GArgs A, int64_t n)
     }
     int64_t t, a, b;
     if (!item_range(A.tp, blockIdx.x, t, a, b)) return;
-    p2g_item<ORDER, LPP>(A, t, a, b, smem, stage_base);
+    p2g_item<ORDER, LPP, REC>(A, t, a, b, smem, stage_base);
 }
 
-template <int ORDER, bool ADV>
+template <int ORDER, bool ADV, bool REC>
 __global__ void __launch_bounds__(G2PThreads<ORDER>::value) g2p_tiled_kernel(G2PArgs A, int64_t n)
 {
     extern __shared__ __align__(16) float smem[];
@@ -44,8 +44,9 @@ __global__ void __launch_bounds__(G2PThreads<ORDER>::value) g2p_tiled_kernel(G2P
     }
     int64_t t, a, b;
     if (!item_range(A.tp, blockIdx.x, t, a, b)) return;  // CTA-uniform
-    g2p_item<ORDER, G2PThreads<ORDER>::value, ADV>(A, t, a, b, reinterpret_cast<float4*>(smem),
-                                                  threadIdx.x);
+    g2p_item<ORDER, G2PThreads<ORDER>::value, ADV, REC>(A, t, a, b,
+                                                       reinterpret_cast<float4*>(smem),
+                                                       threadIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -176,8 +177,12 @@ bool make_tilep(const MeshP& mp, int order, const picasso_bins& bins, TileP* tp,
         tp->nt[d] = bins.num_tiles[d];
         tp->nb[d] = nb;
         tp->NT[d] = bins.tile[d] + K - 1;
+        tp->tsh[d] = -1;
+        for (int sh = 0; sh < 31; ++sh)
+            if ((1 << sh) == bins.tile[d]) tp->tsh[d] = sh;
         nt *= bins.num_tiles[d];
     }
+    tp->tsize = (uint32_t)bins.tile[0] * (uint32_t)bins.tile[1] * (uint32_t)bins.tile[2];
     tp->nodes = tp->NT[0] * tp->NT[1] * tp->NT[2];
     if (lpp > 0) {
         // the accumulator split of p2g_item (P2GCfg::ISPLIT, F)
@@ -217,10 +222,12 @@ bool packed_c(const PField& c)
            (reinterpret_cast<uintptr_t>(c.data) % 16) == 0;
 }
 
-size_t p2g_warp_bytes(int order, int lpp, int P)
+size_t p2g_warp_bytes(int order, int lpp, int P, bool rec)
 {
-#define PB_CASE(O, L) \
-    if (order == O && lpp == L) return sizeof(float) * (size_t)p2g_warp_floats<O, L>(P);
+#define PB_CASE(O, L)                                                                   \
+    if (order == O && lpp == L)                                                         \
+        return sizeof(float) * (size_t)(rec ? p2g_warp_floats<O, L, true>(P)            \
+                                            : p2g_warp_floats<O, L, false>(P));
     PB_CASE(1, 1) PB_CASE(1, 2) PB_CASE(1, 4)
     PB_CASE(2, 1) PB_CASE(2, 2) PB_CASE(2, 4)
     PB_CASE(3, 4)
@@ -233,27 +240,35 @@ static int64_t item_bound(const TileP& tp, int64_t n)
     return tp.ntiles + (n + tp.chunk - 1) / tp.chunk;
 }
 
-template <int ORDER, int LPP>
+template <int ORDER, int LPP, bool REC>
 static picasso_status launch_p2g_tiled(const P2GArgs& A, int64_t n, cudaStream_t st)
 {
-    const size_t smem = p2g_warp_bytes(ORDER, LPP, A.tp.P);
-    PB_CUDA_TRY(cudaFuncSetAttribute(p2g_tiled_kernel<ORDER, LPP>,
+    const size_t smem = p2g_warp_bytes(ORDER, LPP, A.tp.P, REC);
+    PB_CUDA_TRY(cudaFuncSetAttribute(p2g_tiled_kernel<ORDER, LPP, REC>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int64_t items = item_bound(A.tp, n);
-    p2g_tiled_kernel<ORDER, LPP><<<(unsigned)(items ? items : 1), 32, smem, st>>>(A, n);
+    p2g_tiled_kernel<ORDER, LPP, REC><<<(unsigned)(items ? items : 1), 32, smem, st>>>(A, n);
     return check_launch();
 }
 
-template <int ORDER, bool ADV>
+template <int ORDER, bool ADV, bool REC>
 static picasso_status launch_g2p_tiled(const G2PArgs& A, int64_t n, cudaStream_t st)
 {
     const size_t smem = sizeof(float4) * (size_t)A.tp.nodes;
-    PB_CUDA_TRY(cudaFuncSetAttribute(g2p_tiled_kernel<ORDER, ADV>,
+    PB_CUDA_TRY(cudaFuncSetAttribute(g2p_tiled_kernel<ORDER, ADV, REC>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int64_t items = item_bound(A.tp, n);
-    g2p_tiled_kernel<ORDER, ADV>
+    g2p_tiled_kernel<ORDER, ADV, REC>
         <<<(unsigned)(items ? items : 1), G2PThreads<ORDER>::value, smem, st>>>(A, n);
     return check_launch();
+}
+
+// Spline records the tiled kernels may read instead of the positions: a
+// 16-byte aligned array, when the bins carry one.
+static const float* bins_records(const picasso_bins& bins)
+{
+    const uintptr_t r = reinterpret_cast<uintptr_t>(bins.records);
+    return (r && r % 16 == 0) ? static_cast<const float*>(bins.records) : nullptr;
 }
 
 picasso_status apic_p2g_tiled(const MeshP& mp, int order, int ncomp, Form form, int64_t n,
@@ -268,7 +283,9 @@ picasso_status apic_p2g_tiled(const MeshP& mp, int order, int ncomp, Form form, 
     if (!valid_lpp(order, lpp)) return PICASSO_ERR_INVALID_ARGUMENT;
     P2GArgs A;
     if (!make_tilep(mp, order, bins, &A.tp, lpp)) return PICASSO_ERR_INVALID_ARGUMENT;
-    const size_t smem = p2g_warp_bytes(order, lpp, A.tp.P);
+    A.rec = bins_records(bins);
+    const bool rec = A.rec != nullptr;
+    const size_t smem = p2g_warp_bytes(order, lpp, A.tp.P, rec);
     if ((int64_t)smem > device_smem_optin()) return PICASSO_OK;  // tile too large: plain path
     *handled = true;
     A.mp = mp;
@@ -280,8 +297,9 @@ picasso_status apic_p2g_tiled(const MeshP& mp, int order, int ncomp, Form form, 
     A.scale_m = ldexpf(1.f, gm.fixed_bits);
     A.scale_mu = ldexpf(1.f, gmu.fixed_bits);
     A.err = err;
-#define PB_CASE(O, L) \
-    if (order == O && lpp == L) return launch_p2g_tiled<O, L>(A, n, st);
+#define PB_CASE(O, L)                                                                   \
+    if (order == O && lpp == L)                                                         \
+        return rec ? launch_p2g_tiled<O, L, true>(A, n, st) : launch_p2g_tiled<O, L, false>(A, n, st);
     PB_CASE(1, 1) PB_CASE(1, 2) PB_CASE(1, 4)
     PB_CASE(2, 1) PB_CASE(2, 2) PB_CASE(2, 4)
     PB_CASE(3, 4)
@@ -308,14 +326,21 @@ picasso_status apic_g2p_tiled(const MeshP& mp, int order, int ncomp, bool f32, i
     A.err = err;
     A.x_out = adv ? reinterpret_cast<double*>(x.data) : nullptr;
     A.adv = adv ? *adv : Advect{};
+    // the advection needs the positions; without it the records replace them
+    A.rec = adv ? nullptr : reinterpret_cast<const float4*>(bins_records(bins));
     if (adv) {
-        if (order == 1) return launch_g2p_tiled<1, true>(A, n, st);
-        if (order == 2) return launch_g2p_tiled<2, true>(A, n, st);
-        return launch_g2p_tiled<3, true>(A, n, st);
+        if (order == 1) return launch_g2p_tiled<1, true, false>(A, n, st);
+        if (order == 2) return launch_g2p_tiled<2, true, false>(A, n, st);
+        return launch_g2p_tiled<3, true, false>(A, n, st);
     }
-    if (order == 1) return launch_g2p_tiled<1, false>(A, n, st);
-    if (order == 2) return launch_g2p_tiled<2, false>(A, n, st);
-    return launch_g2p_tiled<3, false>(A, n, st);
+    if (A.rec) {
+        if (order == 1) return launch_g2p_tiled<1, false, true>(A, n, st);
+        if (order == 2) return launch_g2p_tiled<2, false, true>(A, n, st);
+        return launch_g2p_tiled<3, false, true>(A, n, st);
+    }
+    if (order == 1) return launch_g2p_tiled<1, false, false>(A, n, st);
+    if (order == 2) return launch_g2p_tiled<2, false, false>(A, n, st);
+    return launch_g2p_tiled<3, false, false>(A, n, st);
 }
 
 }  // namespace pb

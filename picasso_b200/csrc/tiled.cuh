@@ -44,6 +44,8 @@ struct TileP {
     int P;       // that a merge's stencil nodes hit distinct banks; P = stride
                  // between the 4 field planes
     int chunk;
+    int tsh[3];      // log2(T[d]) when T[d] is a power of two, else -1
+    uint32_t tsize;  // bins per tile (sort keys of tile t start at t * tsize)
     int64_t ntiles;
     const int64_t* off;     // tile particle offsets (ntiles + 1)
     const uint32_t* items;  // tile work-item prefix (ntiles + 1)
@@ -54,6 +56,7 @@ struct P2GArgs {
     MeshP mp;
     TileP tp;
     const double* x;
+    const float* rec;  // spline records (4 floats per particle) or null
     const float* m;
     const float* c;
     GField gm;
@@ -67,6 +70,7 @@ struct G2PArgs {
     MeshP mp;
     TileP tp;
     const double* x;
+    const float4* rec;  // spline records or null
     GField u;
     float* c;
     int* err;
@@ -171,16 +175,24 @@ __device__ __forceinline__ void cp_async_wait()
 // P2G
 // ---------------------------------------------------------------------------
 // Shared-memory layout of one P2G warp: particle-record ring, staging area,
-// node tile.  Field g of a node (a, b, c) of a bin receives
-//   w_abc * (c0 + cx dist_a + cy dist_b + cz dist_c)        (order 2 / 3)
+// node tile.  Field g of a node n = (a, b, c) of a bin receives
+//   w_n m (e_d + sum_q G_dq (n_q - n0))                     (order 2 / 3)
 //   m * (c0 www + cx gww + cy wgw + cz wwg)                  (order 1)
-// with (c0, cx, cy, cz) = (1, 0, 0, 0) for the mass (g = 0) and
-// (v_d, D B_d0, D B_d1, D B_d2) for momentum component d = g - 1
-// (APIC.hpp:110-139; order 1: APIC.hpp:287-318 with D = 1).
-template <int ORDER, int LPP>
+// for the momentum components d = g - 1 and w_n m for the mass (g = 0), with
+// n0 the stencil's centre knot, e_d = v_d + D sum_q B_dq dist_q(n0) and
+// G_dq = D dx B_dq: the affine term D B dist (APIC.hpp:110-139) written
+// relative to the centre knot, where dist_q(n) - dist_q(n0) = (n_q - n0) dx,
+// so the nodes next to the centre need one addition and the centre none.
+// Order 1: APIC.hpp:287-318 with D = 1.
+//
+// REC: the particle's position arrives as a spline record (in-cell fraction
+// of the logical position along each dimension in FP32, and the sort key
+// of its bin) instead of the FP64 position.
+template <int ORDER, int LPP, bool REC = false>
 struct P2GCfg {
     static constexpr int K = SplineTraits<ORDER>::K;
     static constexpr int KKK = K * K * K;
+    static constexpr int N0 = 1;  // centre knot of the quadratic and cubic stencils
     // Cubic stencils with 4 lanes per particle split the stencil by its
     // i-planes (lane h sums all four fields of the 16 nodes (h, j, k)); the
     // other splits are by field (lane h sums fields h F .. h F + F - 1 of all
@@ -204,9 +216,12 @@ struct P2GCfg {
     static constexpr int PS = ((PV4 / 4) % 2 == 0) ? PV4 + 4 : PV4;
     static constexpr int RP = (PV + 31) / 32;
     static_assert(PS <= SS, "a plane stages inside a full stage slot");
-    // ring per stage: x (6 floats) | c (12 floats) | m (1 float) per run
-    static constexpr int RING_X = 0, RING_C = 6 * RUNS, RING_M = 18 * RUNS;
-    static constexpr int RING = 19 * RUNS + ((19 * RUNS) % 4 ? 4 - (19 * RUNS) % 4 : 0);
+    // ring per stage: position (6 floats: 3 doubles; REC: one 16-byte
+    // record) | c (12 floats) | m (1 float) per run
+    static constexpr int XS = REC ? 4 : 6;
+    static constexpr int RING_X = 0, RING_C = XS * RUNS, RING_M = (XS + 12) * RUNS;
+    static constexpr int RING =
+        (XS + 13) * RUNS + (((XS + 13) * RUNS) % 4 ? 4 - ((XS + 13) * RUNS) % 4 : 0);
     // ring depth: records of DEPTH - 1 particles are in flight per run; the
     // warps with fewer runs (more lanes per particle) need more to keep the
     // same bytes in flight.  Deeper rings cost shared memory, which costs
@@ -227,10 +242,20 @@ struct P2GOccupancy {
     static constexpr int value = LPP == 1 ? 8 : (LPP == 2 ? 12 : (ORDER == 3 ? 12 : 16));
 };
 
-template <int ORDER, int LPP>
+template <int ORDER, int LPP, bool REC = false>
 __host__ __device__ constexpr int p2g_warp_floats(int P)
 {
-    return P2GCfg<ORDER, LPP>::TILE_OFF + 4 * P;
+    return P2GCfg<ORDER, LPP, REC>::TILE_OFF + 4 * P;
+}
+
+// p + s g for a small integer s (s = 0: p exactly).  Called with unrolled
+// loop indices, so the branch folds at compile time.
+__device__ __forceinline__ float add_steps(int s, float p, float g)
+{
+    if (s == 0) return p;
+    if (s == 1) return p + g;
+    if (s == -1) return p - g;
+    return fmaf((float)s, g, p);
 }
 
 template <int ORDER, int LPP>
@@ -246,30 +271,34 @@ struct P2GAcc {
             for (int n = 0; n < C::NL; ++n) acc[f][n] = 0.f;
     }
 
-    // h: the lane's share of the particle (its i-plane when C::ISPLIT)
+    // Orders 2 / 3.  E[f], G[f][q]: the centre-knot form of field f of the
+    // lane (mass: E = 1, G = 0); h: the lane's share of the particle (its
+    // i-plane when C::ISPLIT).  `mass_first`: field 0 of the lane is the
+    // mass (known at compile time for one lane per particle and for the
+    // plane split).
     __device__ __forceinline__ void add(const Spline1D<ORDER, float> sp[3], float mass,
-                                        const float co[C::F][4], int h)
+                                        const float E[C::F], const float G[C::F][3], int h)
     {
         constexpr int K = C::K;
+        constexpr int N0 = C::N0;
+        constexpr bool MASS0 = C::ISPLIT || LPP == 1;
         if constexpr (C::ISPLIT) {
-            // node (h, j, k): w = wx_h wy_j wz_k m, field g = 1..3 receives
-            // w (c0 + cx dist_h + cy dist_j + cz dist_k), the mass w
-            float wx = 0.f, dx = 0.f;
+            // node (h, j, k): w = wx_h wy_j wz_k m
+            float wx = 0.f;
 #pragma unroll
             for (int i = 0; i < K; ++i)
-                if (i == h) {
-                    wx = sp[0].w[i];
-                    dx = sp[0].d[i];
-                }
-            float e[3];
+                if (i == h) wx = sp[0].w[i];
+            const float wxm = wx * mass;
+            const float hs = (float)(h - N0);
+            float pi[4];
 #pragma unroll
-            for (int f = 1; f < 4; ++f) e[f - 1] = co[f][0] + co[f][1] * dx;
+            for (int f = 1; f < 4; ++f) pi[f] = fmaf(hs, G[f][0], E[f]);
 #pragma unroll
             for (int j = 0; j < K; ++j) {
-                const float wij = wx * sp[1].w[j] * mass;
-                float pij[3];
+                const float wij = wxm * sp[1].w[j];
+                float pij[4];
 #pragma unroll
-                for (int f = 1; f < 4; ++f) pij[f - 1] = e[f - 1] + co[f][2] * sp[1].d[j];
+                for (int f = 1; f < 4; ++f) pij[f] = add_steps(j - N0, pi[f], G[f][1]);
 #pragma unroll
                 for (int k = 0; k < K; ++k) {
                     const int n = j * K + k;
@@ -277,51 +306,63 @@ struct P2GAcc {
                     acc[0][n] += w;
 #pragma unroll
                     for (int f = 1; f < 4; ++f)
-                        acc[f][n] += w * (pij[f - 1] + co[f][3] * sp[2].d[k]);
+                        acc[f][n] = fmaf(w, add_steps(k - N0, pij[f], G[f][2]), acc[f][n]);
                 }
             }
-        } else if (ORDER >= 2) {
+        } else {
 #pragma unroll
-            for (int i = 0; i < K; ++i)
+            for (int i = 0; i < K; ++i) {
+                const float wi = sp[0].w[i] * mass;
+                float pi[C::F];
+#pragma unroll
+                for (int f = 0; f < C::F; ++f) pi[f] = add_steps(i - N0, E[f], G[f][0]);
 #pragma unroll
                 for (int j = 0; j < K; ++j) {
-                    const float wij = sp[0].w[i] * sp[1].w[j] * mass;
+                    const float wij = wi * sp[1].w[j];
                     float pij[C::F];
 #pragma unroll
-                    for (int f = 0; f < C::F; ++f)
-                        pij[f] = co[f][0] + co[f][1] * sp[0].d[i] + co[f][2] * sp[1].d[j];
+                    for (int f = 0; f < C::F; ++f) pij[f] = add_steps(j - N0, pi[f], G[f][1]);
 #pragma unroll
                     for (int k = 0; k < K; ++k) {
                         const int n = (i * K + j) * K + k;
                         const float w = wij * sp[2].w[k];
 #pragma unroll
                         for (int f = 0; f < C::F; ++f) {
-                            if (LPP == 1 && f == 0) acc[f][n] += w;  // mass
-                            else acc[f][n] += w * (pij[f] + co[f][3] * sp[2].d[k]);
+                            if (MASS0 && f == 0) acc[f][n] += w;
+                            else
+                                acc[f][n] =
+                                    fmaf(w, add_steps(k - N0, pij[f], G[f][2]), acc[f][n]);
                         }
                     }
                 }
-        } else {
-#pragma unroll
-            for (int i = 0; i < K; ++i)
-#pragma unroll
-                for (int j = 0; j < K; ++j)
-#pragma unroll
-                    for (int k = 0; k < K; ++k) {
-                        const int n = (i * K + j) * K + k;
-                        const float www = sp[0].w[i] * sp[1].w[j] * sp[2].w[k] * mass;
-                        const float gww = sp[0].g[i] * sp[1].w[j] * sp[2].w[k] * mass;
-                        const float wgw = sp[0].w[i] * sp[1].g[j] * sp[2].w[k] * mass;
-                        const float wwg = sp[0].w[i] * sp[1].w[j] * sp[2].g[k] * mass;
-#pragma unroll
-                        for (int f = 0; f < C::F; ++f) {
-                            if (LPP == 1 && f == 0) acc[f][n] += www;  // mass
-                            else
-                                acc[f][n] += co[f][0] * www + co[f][1] * gww + co[f][2] * wgw +
-                                             co[f][3] * wwg;
-                        }
-                    }
+            }
         }
+    }
+
+    // Order 1 (gradient form); co[f] = (c0, cx, cy, cz) of field f.
+    __device__ __forceinline__ void add_linear(const Spline1D<ORDER, float> sp[3], float mass,
+                                               const float co[C::F][4])
+    {
+        constexpr int K = C::K;
+#pragma unroll
+        for (int i = 0; i < K; ++i)
+#pragma unroll
+            for (int j = 0; j < K; ++j)
+#pragma unroll
+                for (int k = 0; k < K; ++k) {
+                    const int n = (i * K + j) * K + k;
+                    const float www = sp[0].w[i] * sp[1].w[j] * sp[2].w[k] * mass;
+                    const float gww = sp[0].g[i] * sp[1].w[j] * sp[2].w[k] * mass;
+                    const float wgw = sp[0].w[i] * sp[1].g[j] * sp[2].w[k] * mass;
+                    const float wwg = sp[0].w[i] * sp[1].w[j] * sp[2].g[k] * mass;
+#pragma unroll
+                    for (int f = 0; f < C::F; ++f) {
+                        if (LPP == 1 && f == 0) acc[f][n] += www;  // mass
+                        else
+                            acc[f][n] += co[f][0] * www + co[f][1] * gww + co[f][2] * wgw +
+                                         co[f][3] * wwg;
+                    }
+                }
     }
 
     // st[f * FS + n] <- acc[f][n] with 16-byte stores.
@@ -501,15 +542,54 @@ __device__ __forceinline__ void merge_plane(unsigned mask, P2GAcc<ORDER, LPP>& a
     }
 }
 
+// Bin inside tile t of a particle from its sort key; false if the key is
+// not one of the tile's bins (another tile, or outside the mesh).
+__device__ __forceinline__ bool bin_of_key(const TileP& tp, int64_t t, uint32_t key, int lb[3])
+{
+    const uint32_t ll = key - (uint32_t)t * tp.tsize;
+    uint32_t r;
+    if (tp.tsh[2] >= 0) {
+        lb[2] = (int)(ll & (uint32_t)(tp.T[2] - 1));
+        r = ll >> tp.tsh[2];
+    } else {
+        r = ll / (uint32_t)tp.T[2];
+        lb[2] = (int)(ll - r * (uint32_t)tp.T[2]);
+    }
+    if (tp.tsh[1] >= 0) {
+        lb[1] = (int)(r & (uint32_t)(tp.T[1] - 1));
+        lb[0] = (int)(r >> tp.tsh[1]);
+    } else {
+        const uint32_t r2 = r / (uint32_t)tp.T[1];
+        lb[1] = (int)(r - r2 * (uint32_t)tp.T[1]);
+        lb[0] = (int)r2;
+    }
+    return ll < tp.tsize;
+}
+
+// Spline of a particle from its record (in-cell fractions, key) and its bin
+// inside tile t; false if the particle is not in this tile.
+template <int ORDER>
+__device__ __forceinline__ bool locate_record(const MeshP& mp, const TileP& tp, int64_t t,
+                                              float4 r, Spline1D<ORDER, float> sp[3], int lb[3])
+{
+    const bool ok = bin_of_key(tp, t, __float_as_uint(r.w), lb);
+    spline_from_frac<ORDER, float>(r.x, (float)mp.dx[0], mp.rdx[0], sp[0]);
+    spline_from_frac<ORDER, float>(r.y, (float)mp.dx[1], mp.rdx[1], sp[1]);
+    spline_from_frac<ORDER, float>(r.z, (float)mp.dx[2], mp.rdx[2], sp[2]);
+    return ok;
+}
+
 // One P2G work item (tile t, particles [a, b)) by the calling warp.  `warp_smem`
-// holds p2g_warp_floats(P) floats (16-byte aligned), `stage_base` kStageLanes
-// ints of shared memory.
-template <int ORDER, int LPP>
+// holds p2g_warp_floats<ORDER, LPP, REC>(P) floats (16-byte aligned),
+// `stage_base` kStageLanes ints of shared memory.
+template <int ORDER, int LPP, bool REC = false>
 __device__ void p2g_item(const P2GArgs& A, int64_t t, int64_t a, int64_t b, float* warp_smem,
                          int* stage_base)
 {
-    using C = P2GCfg<ORDER, LPP>;
+    using C = P2GCfg<ORDER, LPP, REC>;
     using Acc = P2GAcc<ORDER, LPP>;
+    static_assert(C::SV == P2GCfg<ORDER, LPP>::SV && C::SS == P2GCfg<ORDER, LPP>::SS,
+                  "the record form changes only the ring");
     constexpr int K = C::K;
     const MeshP& mp = A.mp;
     const TileP& tp = A.tp;
@@ -524,27 +604,57 @@ __device__ void p2g_item(const P2GArgs& A, int64_t t, int64_t a, int64_t b, floa
     const int U = (int)((b - a + C::RUNS - 1) / C::RUNS);
     const int64_t my0 = a + (int64_t)run * U;
     const int cnt = (int)max((int64_t)0, min(my0 + U, b) - my0);
+    // bin rows spanned by the item (keys are i-major within a tile): the
+    // first and last particle bound them; the item's node box is these rows
+    // plus the halo, over the whole tile along j and k
+    int i_lo = 0, i_hi = tp.T[0] - 1;
+    {
+        int la[3], lz[3];
+        bool oka, okb;
+        if constexpr (REC) {
+            oka = bin_of_key(tp, t, __float_as_uint(__ldg(A.rec + 4 * a + 3)), la);
+            okb = bin_of_key(tp, t, __float_as_uint(__ldg(A.rec + 4 * (b - 1) + 3)), lz);
+        } else {
+            Spline1D<ORDER, float> sp[3];
+            const double xa[3] = {A.x[3 * a], A.x[3 * a + 1], A.x[3 * a + 2]};
+            const double xb[3] = {A.x[3 * (b - 1)], A.x[3 * (b - 1) + 1], A.x[3 * (b - 1) + 2]};
+            oka = locate<ORDER>(mp, tp, xa, ob, sp, la);
+            okb = locate<ORDER>(mp, tp, xb, ob, sp, lz);
+        }
+        if (oka && okb && lz[0] >= la[0]) {
+            i_lo = la[0];
+            i_hi = lz[0];
+        }
+    }
 
     for (int i = lane; i < 4 * tp.P; i += 32) tile[i] = 0.f;
     MergePlan<ORDER, LPP> plan;
     plan.init(tp, lane);
     const float D = (ORDER >= 2) ? inertial_scaling<ORDER, float>(mp.dx[0]) : 1.f;
+    const float Dh = D * (float)mp.dx[0];
 
     auto slot = [&](int q) { return ring + (q % C::DEPTH) * C::RING; };
-    // the 7 copies of a particle record (x0..x2, c0..c2, m) are spread over
-    // the run's lanes: copy j is issued by lane h == j % LPP
+    // the copies of a particle record are spread over the run's lanes: copy
+    // j is issued by lane h == j % LPP (position: 3 x 8 bytes or one 16-byte
+    // record, c: 3 x 16 bytes, m: 4 bytes)
+    constexpr int NX = REC ? 1 : 3;
     auto issue = [&](int q) {
         if (q < cnt) {
             const int64_t p = my0 + q;
             float* s = slot(q);
-            float* sx = s + C::RING_X + run * 6;
+            float* sx = s + C::RING_X + run * C::XS;
             float* sc = s + C::RING_C + run * 12;
 #pragma unroll
-            for (int j = 0; j < 7; ++j) {
+            for (int j = 0; j < NX + 4; ++j) {
                 if (j % LPP != h) continue;
-                if (j < 3) cp_async<8>(sx + 2 * j, A.x + 3 * p + j);
-                else if (j < 6) cp_async<16>(sc + 4 * (j - 3), A.c + 12 * p + 4 * (j - 3));
-                else cp_async<4>(s + C::RING_M + run, A.m + p);
+                if (j < NX) {
+                    if constexpr (REC) cp_async<16>(sx, A.rec + 4 * p);
+                    else cp_async<8>(sx + 2 * j, A.x + 3 * p + j);
+                } else if (j < NX + 3) {
+                    cp_async<16>(sc + 4 * (j - NX), A.c + 12 * p + 4 * (j - NX));
+                } else {
+                    cp_async<4>(s + C::RING_M + run, A.m + p);
+                }
             }
         }
         cp_async_commit();
@@ -563,15 +673,22 @@ __device__ void p2g_item(const P2GArgs& A, int64_t t, int64_t a, int64_t b, floa
         P.ok = false;
         P.lb[0] = P.lb[1] = P.lb[2] = 0;
         if (q >= cnt) return;
-        const double* sx = reinterpret_cast<const double*>(slot(q) + C::RING_X + run * 6);
-        const double xp[3] = {sx[0], sx[1], sx[2]};
-        P.ok = locate<ORDER>(mp, tp, xp, ob, P.sp, P.lb);
+        if constexpr (REC) {
+            const float4 r = *reinterpret_cast<const float4*>(slot(q) + C::RING_X + run * 4);
+            P.ok = locate_record<ORDER>(mp, tp, t, r, P.sp, P.lb);
+        } else {
+            const double* sx = reinterpret_cast<const double*>(slot(q) + C::RING_X + run * 6);
+            const double xp[3] = {sx[0], sx[1], sx[2]};
+            P.ok = locate<ORDER>(mp, tp, xp, ob, P.sp, P.lb);
+        }
+        // a particle out of the item's rows (the particles are not sorted)
+        // is skipped like one of another tile
+        P.ok = P.ok && P.lb[0] >= i_lo && P.lb[0] <= i_hi;
         if (!P.ok && A.err && h == 0) atomicAdd(A.err, 1);
     };
-    auto coefficients = [&](int q, float co[C::F][4], float& mass) {
+    auto read_c = [&](int q, float cp[12], float& mass) {
         const float* sl = slot(q);
         const float* sc = sl + C::RING_C + run * 12;
-        float cp[12];  // cp[r * 3 + d] = c_p(r, d)
 #pragma unroll
         for (int v = 0; v < 3; ++v) {
             const float4 w = *reinterpret_cast<const float4*>(sc + 4 * v);
@@ -581,18 +698,45 @@ __device__ void p2g_item(const P2GArgs& A, int64_t t, int64_t a, int64_t b, floa
             cp[4 * v + 3] = w.w;
         }
         mass = sl[C::RING_M + run];
+    };
+    // cp[r * 3 + d] = c_p(r, d); field g of the lane: mass (g = 0) or
+    // momentum d = g - 1
+    auto centre_form = [&](const float cp[12], const Spline1D<ORDER, float> sp[3],
+                           float E[C::F], float G[C::F][3]) {
 #pragma unroll
         for (int f = 0; f < C::F; ++f) {
-            const int g = C::ISPLIT ? f : h * C::F + f;  // global field
+            const int g = C::ISPLIT ? f : h * C::F + f;
+            if (g == 0) {
+                E[f] = 1.f;
+                G[f][0] = G[f][1] = G[f][2] = 0.f;
+            } else {
+                const int d = g - 1;
+                const float bx = d == 0 ? cp[3] : (d == 1 ? cp[4] : cp[5]);
+                const float by = d == 0 ? cp[6] : (d == 1 ? cp[7] : cp[8]);
+                const float bz = d == 0 ? cp[9] : (d == 1 ? cp[10] : cp[11]);
+                const float v = d == 0 ? cp[0] : (d == 1 ? cp[1] : cp[2]);
+                const float bd = fmaf(bz, sp[2].d[C::N0],
+                                      fmaf(by, sp[1].d[C::N0], bx * sp[0].d[C::N0]));
+                E[f] = fmaf(D, bd, v);
+                G[f][0] = Dh * bx;
+                G[f][1] = Dh * by;
+                G[f][2] = Dh * bz;
+            }
+        }
+    };
+    auto linear_form = [&](const float cp[12], float co[C::F][4]) {
+#pragma unroll
+        for (int f = 0; f < C::F; ++f) {
+            const int g = h * C::F + f;
             if (g == 0) {
                 co[f][0] = 1.f;
                 co[f][1] = co[f][2] = co[f][3] = 0.f;
             } else {
                 const int d = g - 1;
                 co[f][0] = d == 0 ? cp[0] : (d == 1 ? cp[1] : cp[2]);
-                co[f][1] = D * (d == 0 ? cp[3] : (d == 1 ? cp[4] : cp[5]));
-                co[f][2] = D * (d == 0 ? cp[6] : (d == 1 ? cp[7] : cp[8]));
-                co[f][3] = D * (d == 0 ? cp[9] : (d == 1 ? cp[10] : cp[11]));
+                co[f][1] = d == 0 ? cp[3] : (d == 1 ? cp[4] : cp[5]);
+                co[f][2] = d == 0 ? cp[6] : (d == 1 ? cp[7] : cp[8]);
+                co[f][3] = d == 0 ? cp[9] : (d == 1 ? cp[10] : cp[11]);
             }
         }
     };
@@ -600,7 +744,6 @@ __device__ void p2g_item(const P2GArgs& A, int64_t t, int64_t a, int64_t b, floa
     Acc acc;
     acc.zero();
     int cur = -1, cur_base = 0;
-    int bmin[3] = {1 << 30, 1 << 30, 1 << 30}, bmax[3] = {-1, -1, -1};
     for (int s = 0; s < U; ++s) {
         __syncwarp();  // no lane still reads the slot refilled next
         issue(s + C::DEPTH - 1);
@@ -623,37 +766,32 @@ __device__ void p2g_item(const P2GArgs& A, int64_t t, int64_t a, int64_t b, floa
             if (lbin != cur) {
                 cur = lbin;
                 cur_base = lb[0] * tp.SI + lb[1] * tp.SJ + lb[2];
-#pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    bmin[d] = min(bmin[d], lb[d]);
-                    bmax[d] = max(bmax[d], lb[d]);
-                }
             }
-            float co[C::F][4], mass;
-            coefficients(s, co, mass);
-            acc.add(P.sp, mass, co, h);
+            float cp[12], mass;
+            read_c(s, cp, mass);
+            if constexpr (ORDER >= 2) {
+                float E[C::F], G[C::F][3];
+                centre_form(cp, P.sp, E, G);
+                acc.add(P.sp, mass, E, G, h);
+            } else {
+                float co[C::F][4];
+                linear_form(cp, co);
+                acc.add_linear(P.sp, mass, co);
+            }
         }
     }
     cp_async_wait<0>();
     const unsigned fm = __ballot_sync(kFull, cur >= 0);
     if (fm) merge_partials<ORDER, LPP>(fm, acc, cur_base, plan, tile, stage, stage_base, lane);
-    // touched node box, rounded to fixed point and added to HBM
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            bmin[d] = min(bmin[d], __shfl_xor_sync(kFull, bmin[d], o));
-            bmax[d] = max(bmax[d], __shfl_xor_sync(kFull, bmax[d], o));
-        }
-    }
-    if (bmax[0] >= 0) {
-        const int e0 = bmax[0] - bmin[0] + K, e1 = bmax[1] - bmin[1] + K;
-        const int e2 = bmax[2] - bmin[2] + K;
-        const int total = e0 * e1 * e2;
+    // the item's node box, rounded to fixed point and added to HBM (nodes
+    // that received nothing are skipped)
+    if (__any_sync(kFull, cur >= 0)) {
+        const int e1 = tp.NT[1], e2 = tp.NT[2];
+        const int total = (i_hi - i_lo + K) * e1 * e2;
         for (int e = lane; e < total; e += 32) {
-            const int k = bmin[2] + e % e2;
-            const int j = bmin[1] + (e / e2) % e1;
-            const int i = bmin[0] + e / (e1 * e2);
+            const int k = e % e2;
+            const int j = (e / e2) % e1;
+            const int i = i_lo + e / (e1 * e2);
             const int idx = i * tp.SI + j * tp.SJ + k;
             const int gi = node_global(mp, tp, 0, ob[0], i);
             const int gj = node_global(mp, tp, 1, ob[1], j);
@@ -683,11 +821,14 @@ __device__ void p2g_item(const P2GArgs& A, int64_t t, int64_t a, int64_t b, floa
 // ADV: each particle is then moved, x += dt u_p (FP64, as picasso_advect).
 // The positions of the item's first and last particle are read before the
 // tile barrier, so no thread reads a position another thread has moved.
-template <int ORDER, int NTHR, bool ADV = false>
+// REC: the particles' splines come from their records (not with ADV).
+template <int ORDER, int NTHR, bool ADV = false, bool REC = false>
 __device__ void g2p_item(const G2PArgs& A, int64_t t, int64_t a, int64_t b, float4* tile,
                          int tid)
 {
+    static_assert(!(ADV && REC), "the advection reads the FP64 positions");
     constexpr int K = SplineTraits<ORDER>::K;
+    constexpr int N0 = ORDER == 1 ? 0 : 1;  // centre knot of the stencil
     const MeshP& mp = A.mp;
     const TileP& tp = A.tp;
     auto sync = [] {
@@ -699,7 +840,15 @@ __device__ void g2p_item(const G2PArgs& A, int64_t t, int64_t a, int64_t b, floa
     // bin rows spanned by the item: the first and last particle bound the
     // slowest tile dimension (keys are i-major within a tile)
     int i_lo = 0, i_hi = tp.T[0] - 1;
-    {
+    if constexpr (REC) {
+        int la[3], lz[3];
+        const bool oka = bin_of_key(tp, t, __float_as_uint(__ldg(&A.rec[a].w)), la);
+        const bool okb = bin_of_key(tp, t, __float_as_uint(__ldg(&A.rec[b - 1].w)), lz);
+        if (oka && okb && lz[0] >= la[0]) {
+            i_lo = la[0];
+            i_hi = lz[0];
+        }
+    } else {
         Spline1D<ORDER, float> sp[3];
         int lb[3];
         const double xa[3] = {A.x[3 * a], A.x[3 * a + 1], A.x[3 * a + 2]};
@@ -734,37 +883,50 @@ __device__ void g2p_item(const G2PArgs& A, int64_t t, int64_t a, int64_t b, floa
         tile[(i * tp.NT[1] + j) * tp.NT[2] + k] = v;
     }
     sync();
-    // positions are prefetched one particle ahead
+    // positions (records) are prefetched one particle ahead
     double xn[3] = {0.0, 0.0, 0.0};
+    float4 rn = make_float4(0.f, 0.f, 0.f, 0.f);
     if (a + tid < b) {
         const int64_t p0 = a + tid;
-        xn[0] = A.x[3 * p0];
-        xn[1] = A.x[3 * p0 + 1];
-        xn[2] = A.x[3 * p0 + 2];
+        if constexpr (REC) {
+            rn = __ldg(A.rec + p0);
+        } else {
+            xn[0] = A.x[3 * p0];
+            xn[1] = A.x[3 * p0 + 1];
+            xn[2] = A.x[3 * p0 + 2];
+        }
     }
     for (int64_t p = a + tid; p < b; p += NTHR) {
         const double xp[3] = {xn[0], xn[1], xn[2]};
+        const float4 rp = rn;
         const int64_t pn = p + NTHR;
         if (pn < b) {
-            xn[0] = A.x[3 * pn];
-            xn[1] = A.x[3 * pn + 1];
-            xn[2] = A.x[3 * pn + 2];
+            if constexpr (REC) {
+                rn = __ldg(A.rec + pn);
+            } else {
+                xn[0] = A.x[3 * pn];
+                xn[1] = A.x[3 * pn + 1];
+                xn[2] = A.x[3 * pn + 2];
+            }
         }
         Spline1D<ORDER, float> sp[3];
         int lb[3];
-        if (!locate<ORDER>(mp, tp, xp, ob, sp, lb) || lb[0] < i_lo || lb[0] > i_hi) {
+        bool ok;
+        if constexpr (REC) ok = locate_record<ORDER>(mp, tp, t, rp, sp, lb);
+        else ok = locate<ORDER>(mp, tp, xp, ob, sp, lb);
+        if (!ok || lb[0] < i_lo || lb[0] > i_hi) {
             if (A.err) atomicAdd(A.err, 1);
             continue;
         }
         const int base = (lb[0] * tp.NT[1] + lb[1]) * tp.NT[2] + lb[2];
-        // APIC.hpp:439-461, contracted one dimension at a time:
+        // APIC.hpp:439-461, contracted one dimension at a time, with the
+        // distances relative to the centre knot n0 (dist_q(n) = dist_q(n0)
+        // + (n_q - n0) dx):
         //   u_p      = sum_i wx_i sum_j wy_j sum_k wz_k u_ijk
-        //   B_p(:,q) = sum_ijk w_ijk u_ijk dist_q  (dist_q along x, y or z)
+        //   M_q      = sum_ijk w_ijk u_ijk (n_q - n0)
+        //   B_p(:,q) = dx M_q + dist_q(n0) u_p
         float up[3] = {0.f, 0.f, 0.f};
-        float B[3][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
-        float wzdz[K];
-#pragma unroll
-        for (int k = 0; k < K; ++k) wzdz[k] = sp[2].w[k] * sp[2].d[k];
+        float M[3][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
 #pragma unroll
         for (int i = 0; i < K; ++i) {
             float A0[3] = {0.f, 0.f, 0.f}, A1[3] = {0.f, 0.f, 0.f}, A2[3] = {0.f, 0.f, 0.f};
@@ -778,27 +940,36 @@ __device__ void g2p_item(const G2PArgs& A, int64_t t, int64_t a, int64_t b, floa
                     const float uk[3] = {ue.x, ue.y, ue.z};
 #pragma unroll
                     for (int d = 0; d < 3; ++d) {
-                        S0[d] += sp[2].w[k] * uk[d];
-                        S1[d] += wzdz[k] * uk[d];
+                        const float wu = sp[2].w[k] * uk[d];
+                        S0[d] += wu;
+                        S1[d] = add_steps(k - N0, S1[d], wu);
                     }
                 }
-                const float wy = sp[1].w[j], wydy = wy * sp[1].d[j];
+                const float wy = sp[1].w[j];
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
-                    A0[d] += wy * S0[d];
-                    A1[d] += wydy * S0[d];
-                    A2[d] += wy * S1[d];
+                    const float wS0 = wy * S0[d];
+                    A0[d] += wS0;
+                    A1[d] = add_steps(j - N0, A1[d], wS0);
+                    A2[d] = fmaf(wy, S1[d], A2[d]);
                 }
             }
-            const float wx = sp[0].w[i], wxdx = wx * sp[0].d[i];
+            const float wx = sp[0].w[i];
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
-                up[d] += wx * A0[d];
-                B[d][0] += wxdx * A0[d];
-                B[d][1] += wx * A1[d];
-                B[d][2] += wx * A2[d];
+                const float wA0 = wx * A0[d];
+                up[d] += wA0;
+                M[d][0] = add_steps(i - N0, M[d][0], wA0);
+                M[d][1] = fmaf(wx, A1[d], M[d][1]);
+                M[d][2] = fmaf(wx, A2[d], M[d][2]);
             }
         }
+        float B[3][3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+#pragma unroll
+            for (int q = 0; q < 3; ++q)
+                B[d][q] = fmaf((float)mp.dx[q], M[d][q], sp[q].d[N0] * up[d]);
         // c_p(0, d) = u_p(d); c_p(1 + q, d) = B_p(d, q)  (APIC.hpp:464-471)
         float4* out = reinterpret_cast<float4*>(A.c + 12 * p);
         out[0] = make_float4(up[0], up[1], up[2], B[0][0]);
@@ -819,6 +990,6 @@ bool packed_m(const PField& m);
 bool packed_c(const PField& c);
 int default_lpp(int order);
 bool valid_lpp(int order, int lpp);
-size_t p2g_warp_bytes(int order, int lpp, int P);
+size_t p2g_warp_bytes(int order, int lpp, int P, bool rec = false);
 
 }  // namespace pb
