@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--p2g-lanes", type=int, default=0,
                     help="lanes per particle of the tiled P2G (0 = library choice)")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 plain leg")
+    ap.add_argument("--no-fuse", action="store_true",
+                    help="grid velocity as a separate pass instead of inside the P2G launch")
     ap.add_argument("--no-records", action="store_true",
                     help="tiled kernels read the positions instead of spline records")
     ap.add_argument("--batch-leg-instances", type=int, default=96,
@@ -294,9 +296,12 @@ def config_of(args):
 class Step:
     """Buffers and launches of one form of the APIC step.  With bins that
     carry spline records the tiled kernels read the records instead of the
-    positions (16 instead of 24 bytes per particle and transfer)."""
+    positions (16 instead of 24 bytes per particle and transfer).  fused:
+    the precision form's grid velocity update runs inside the P2G launch
+    (APIC.p2g_update), so the step has no separate velocity pass (its
+    "velocity" interval is empty)."""
 
-    def __init__(self, form, mesh, x, m, c, bins, stream):
+    def __init__(self, form, mesh, x, m, c, bins, stream, fused=False):
         import torch
 
         import picasso_b200 as pb
@@ -323,6 +328,13 @@ class Step:
             self.gmu = self.acc[..., 1:]
             self.u = torch.zeros(ext + (3,), dtype=torch.float64, device=dev)
         self.acc_fill = pb.FixedGrid(self.acc, FIXED_BITS) if form == "fp32" else self.acc
+        self.fused = bool(fused and form == "fp32" and bins is not None)
+        self.ws = None
+        if self.fused:
+            self.ws = torch.empty(pb.p2g_update_workspace(bins), dtype=torch.uint8, device=dev)
+        # memset + kernels of the library per step: fill (memset), P2G,
+        # velocity, G2P; fused: fill, counter memset, empty-region kernel,
+        # P2G + update, G2P
         self.launches_per_step = 4
 
     def run(self, events=None):
@@ -333,12 +345,21 @@ class Step:
         pb.grid_fill(self.desc, self.acc_fill, 0.0, ncomp=4, stream=s)
         if events is not None:
             events[1].record(s)
-        pb.APIC.p2g(self.m, self.c, self.gm, self.gmu, self.sd, stream=s, bins=self.bins)
-        if events is not None:
-            events[2].record(s)
-        pb.grid_velocity(self.desc, self.gm, self.gmu, self.u, 1e-12, stream=s)
-        if events is not None:
-            events[3].record(s)
+        if self.fused:
+            # v = p / m where m > 1e-12 (dt = 0: no force, no gravity)
+            pb.APIC.p2g_update(self.m, self.c, self.gm, self.gmu, self.u, self.sd, dt=0.0,
+                               mass_threshold=1e-12, workspace=self.ws, stream=s,
+                               bins=self.bins)
+            if events is not None:
+                events[2].record(s)
+                events[3].record(s)
+        else:
+            pb.APIC.p2g(self.m, self.c, self.gm, self.gmu, self.sd, stream=s, bins=self.bins)
+            if events is not None:
+                events[2].record(s)
+            pb.grid_velocity(self.desc, self.gm, self.gmu, self.u, 1e-12, stream=s)
+            if events is not None:
+                events[3].record(s)
         pb.APIC.g2p(self.u, self.c, self.sd, stream=s, bins=self.bins)
         if events is not None:
             events[4].record(s)
@@ -356,6 +377,13 @@ class Step:
         else:
             sf, sg, su = 8, 8, 8
         px = 16 if self.records else 24
+        if self.fused:
+            # the update reads the accumulators the P2G has just added into
+            # (L2) and writes the velocity
+            return {"fill": nodes * 4 * sg,
+                    "p2g": n * (px + 13 * sf) + nodes * (4 * sg + 3 * su),
+                    "velocity": 0,
+                    "g2p": n * (px + 12 * sf) + nodes * 3 * su}
         return {"fill": nodes * 4 * sg,
                 "p2g": n * (px + 13 * sf) + nodes * 4 * sg,
                 "velocity": nodes * (4 * sg + 3 * su),
@@ -495,7 +523,8 @@ def run_ours(args):
 
     out = {}
     # FP32 precision form (headline)
-    s32 = Step("fp32", mesh, x, m32, c32.clone(), bins, stream)
+    fused = bins is not None and not args.no_fuse
+    s32 = Step("fp32", mesh, x, m32, c32.clone(), bins, stream, fused=fused)
     clk.start()
     ms32, per32 = time_form(s32, args.steps, args.warmup, dist)
     clocks = clk.stop()
@@ -507,7 +536,7 @@ def run_ours(args):
         # the same step with the tiled kernels reading the FP64 positions
         rec_keep = bins.records
         bins.attach_records(None)
-        sx = Step("fp32", mesh, x, m32, c32.clone(), bins, stream)
+        sx = Step("fp32", mesh, x, m32, c32.clone(), bins, stream, fused=fused)
         msx, perx = time_form(sx, args.steps, args.warmup, dist)
         rfx, _ = roofline(sx, perx, n, nodes, peak)
         from_positions = {"ms_per_step": msx, "particles_per_s": world * n / (msx * 1e-3),
@@ -515,6 +544,14 @@ def run_ours(args):
                           else None}
         del sx
         bins.attach_records(rec_keep)
+    unfused = None
+    if fused:
+        # the same step with the grid velocity as a separate pass
+        sf_ = Step("fp32", mesh, x, m32, c32.clone(), bins, stream, fused=False)
+        msf, perf = time_form(sf_, args.steps, args.warmup, dist)
+        unfused = {"ms_per_step": msf, "particles_per_s": world * n / (msf * 1e-3),
+                   "kernels_ms": perf}
+        del sf_
     # FP64 plain form: on the generation-order particles (no sort, as the
     # reference runs) and on the cell-sorted ones
     if not args.no_fp64:
@@ -588,10 +625,17 @@ def run_ours(args):
                                           and bins.records is not None else "3 x FP64"),
                               "achieved_gbs": n * model_bytes / (ms32 * 1e-3) / 1e9,
                               "frac": n * model_bytes / (ms32 * 1e-3) / 1e9 / peak["hbm_gbs"]},
-            "kernels": k32, "gpu_launches": 4 * args.steps,
+            "kernels": k32,
+            # kernels of this library per step: P2G (+ update), the empty-region
+            # zeroing or the velocity pass, G2P (the fills are cudaMemsetAsync)
+            "gpu_launches": 3 * args.steps,
             "clocks": clocks}
     if from_positions:
         line["fp32_from_positions"] = from_positions
+    if unfused:
+        line["fp32_separate_velocity_pass"] = unfused
+    line["step"] = ("fill (memset), P2G with the grid velocity update fused into its flush, G2P"
+                    if fused else "fill (memset), P2G, grid velocity, G2P")
     if "fp64" in out:
         ms64, per64, rf64, k64 = out["fp64"]
         line["fp64_plain"] = {"value": world * n / (ms64 * 1e-3), "ms_per_step": ms64,
@@ -685,8 +729,10 @@ def run_advect(args, peak):
     dt = 0.1 / g
     seed = 1001
     res = {"workload": "cubic APIC, %d^3 periodic, 8 ppc uniform, dt = 0.1 dx, per step: "
-                       "cell re-sort (from the keys the previous G2P emitted) + permute, fill, P2G, "
-                       "velocity, G2P + advection + sort keys" % g,
+                       "cell re-sort (from the keys the previous G2P emitted) + permute (FP32 "
+                       "form: + spline records of the permuted particles), fill, P2G, "
+                       "velocity (FP32 form: inside the P2G launch), G2P + advection + sort "
+                       "keys" % g,
            "steps": args.adv_steps, "tile": list(args.adv_tile)}
     names = ["sort", "permute", "fill", "p2g", "velocity", "g2p_advect"]
     for form in ("fp64", "fp32"):
@@ -713,6 +759,10 @@ def run_advect(args, peak):
         # timed steps allocate no particle storage
         spare = {"x": torch.empty_like(x), "m": torch.empty_like(m), "c": torch.empty_like(c)}
         sort_bufs = pb.SortBuffers(pb.create_spline(loc, 3, mesh, x), tile)
+        # FP32 form: spline records of the permuted particles for P2G, and the
+        # grid velocity inside the P2G launch
+        recbuf = torch.empty((n, 4), dtype=torch.float32, device="cuda") if f32 else None
+        fws = {}
 
         def step(ev=None):
             def mark(i):
@@ -726,13 +776,23 @@ def run_advect(args, peak):
             for name in ("x", "m", "c"):
                 pb.permute(perm, state[name], spare[name])
                 state[name], spare[name] = spare[name], state[name]
-            mark(2)
             sd = pb.create_spline(loc, 3, mesh, state["x"])
+            if f32:
+                pb.spline_records(sd, bins, out=recbuf)
+            mark(2)
             pb.grid_fill(desc, fill, 0.0, ncomp=4)
             mark(3)
-            pb.APIC.p2g(state["m"], state["c"], gm, gmu, sd, bins=bins)
-            mark(4)
-            pb.grid_velocity(desc, gm, gmu, u, 1e-12)
+            if f32:
+                if "ws" not in fws:
+                    fws["ws"] = torch.empty(pb.p2g_update_workspace(bins), dtype=torch.uint8,
+                                            device="cuda")
+                pb.APIC.p2g_update(state["m"], state["c"], gm, gmu, u, sd, dt=0.0,
+                                   mass_threshold=1e-12, workspace=fws["ws"], bins=bins)
+                mark(4)
+            else:
+                pb.APIC.p2g(state["m"], state["c"], gm, gmu, sd, bins=bins)
+                mark(4)
+                pb.grid_velocity(desc, gm, gmu, u, 1e-12)
             mark(5)
             state["keys"] = pb.APIC.g2p_advect(u, state["c"], sd, dt, bins=bins, key_tile=tile,
                                                keys_out=keybuf)
@@ -755,10 +815,11 @@ def run_advect(args, peak):
         xs = state["x"]
         nodes = g ** 3
         sf = 4 if f32 else 8
-        kb = {"permute": n * (2 * (24 + sf + 12 * sf) + 3 * 4),
+        px = 16 if f32 else 24  # FP32 form: P2G reads the spline records
+        kb = {"permute": n * (2 * (24 + sf + 12 * sf) + 3 * 4 + (24 + 16 if f32 else 0)),
               "fill": nodes * 32,
-              "p2g": n * (24 + 13 * sf) + nodes * 32,
-              "velocity": nodes * (32 + 3 * sf),
+              "p2g": n * (px + 13 * sf) + nodes * (32 + (3 * sf if f32 else 0)),
+              "velocity": 0 if f32 else nodes * (32 + 3 * sf),
               "g2p_advect": n * (24 + 24 + 12 * sf + 4) + nodes * 3 * sf}
         step_bytes = sum(kb.values())
         res[form] = {"ms_per_step": ms, "particles_per_s": n / (ms * 1e-3),

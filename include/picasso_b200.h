@@ -297,6 +297,29 @@ PICASSO_API picasso_status picasso_grid_update(const picasso_mesh* mesh, picasso
                                                picasso_grid_field u_i, picasso_grid_field u64_i,
                                                const picasso_exec* exec);
 
+/* APIC::p2g (collocated, 3 components) followed by the grid update, in one
+ * launch for cell-sorted particles in the precision form: the work items of
+ * the tiled P2G count their arrival at the node regions they touch, and the
+ * item that completes a region converts its nodes with the update of
+ * picasso_grid_update (u = (mu + dt f) / m + dt g, threshold, walls) while
+ * they are still in L2.  Results are bit-identical to picasso_apic_p2g then
+ * picasso_grid_update, which is also what runs when the fused form does not
+ * apply (no bins, FP64 form, staggered location, tiles of fewer than K - 1
+ * bins, F32 velocity not requested).  m_i / mu_i receive the P2G sums as in
+ * picasso_apic_p2g (zero them first); f_i: optional FP64 force; u_i: FP32;
+ * u64_i optional FP64 copy.  `workspace`: device memory of the size
+ * picasso_apic_p2g_update_workspace reports (8 counters per tile), cleared by
+ * the call.  No counterpart in the reference, which leaves the step between
+ * P2G and G2P to the application (doc/basic/explict_nearly_incompressible_flow.md:20-21). */
+PICASSO_API picasso_status picasso_apic_p2g_update_workspace(const picasso_bins* bins,
+                                                             int64_t* bytes);
+PICASSO_API picasso_status picasso_apic_p2g_update(
+    const picasso_spline* sd, int64_t num_particles, picasso_particle_field x_p,
+    picasso_particle_field m_p, picasso_particle_field c_p, picasso_grid_field m_i,
+    picasso_grid_field mu_i, picasso_grid_field f_i, const picasso_grid_update_params* params,
+    picasso_grid_field u_i, picasso_grid_field u64_i, void* workspace, int64_t workspace_bytes,
+    const picasso_exec* exec);
+
 /* Particle advection x_p += dt * c_p(0, :) in FP64, then periodic wrap of the
  * position into the owned box along periodic dimensions. */
 PICASSO_API picasso_status picasso_advect(const picasso_mesh* mesh, int64_t num_particles,

@@ -30,6 +30,7 @@ from .api import (  # noqa: F401
     grid_update,
     grid_velocity,
     mat3_inverse,
+    p2g_update_workspace,
     particle_field,
     permute,
     permute_members,

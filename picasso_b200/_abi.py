@@ -119,6 +119,11 @@ SIGNATURES = [
     ("picasso_grid_update", C.c_int,
      [C.POINTER(Mesh), GridField, GridField, GridField, C.POINTER(GridUpdateParams), GridField,
       GridField, C.POINTER(Exec)]),
+    ("picasso_apic_p2g_update_workspace", C.c_int, [C.POINTER(Bins), C.POINTER(C.c_int64)]),
+    ("picasso_apic_p2g_update", C.c_int,
+     [C.POINTER(Spline), C.c_int64, ParticleField, ParticleField, ParticleField, GridField,
+      GridField, GridField, C.POINTER(GridUpdateParams), GridField, GridField, C.c_void_p,
+      C.c_int64, C.POINTER(Exec)]),
     ("picasso_advect", C.c_int,
      [C.POINTER(Mesh), C.c_int64, C.c_double, ParticleField, ParticleField, C.POINTER(Exec)]),
     ("picasso_apic_g2p_advect", C.c_int,

@@ -312,6 +312,33 @@ class APIC:
                                       C.byref(ex.desc)), "APIC::p2g")
 
     @staticmethod
+    def p2g_update(m_p, c_p, m_i, mu_i, u_i, sd, dt=0.0, gravity=(0.0, 0.0, 0.0), f_i=None,
+                   mass_threshold=1e-12, walls=None, wall_width=1, u64_i=None, workspace=None,
+                   stream=None, error_count=None, bins=None, overflow_count=None):
+        """APIC::p2g followed by the grid update of grid_update (same
+        arguments), fused into one launch for cell-sorted particles in the
+        precision form (picasso_apic_p2g_update; the two separate calls
+        otherwise, with bit-identical results).  `workspace`: a uint8 CUDA
+        tensor of p2g_update_workspace(bins) bytes, allocated if not given."""
+        _check_grid_extent(m_i, sd.desc.mesh)
+        _check_grid_extent(mu_i, sd.desc.mesh)
+        _check_grid_extent(u_i, sd.desc.mesh)
+        if workspace is None and bins is not None:
+            workspace = torch.empty(max(p2g_update_workspace(bins), 1), dtype=torch.uint8,
+                                    device=sd.x.device)
+        prm = _update_params(dt, gravity, mass_threshold, walls, wall_width)
+        ex = _exec(stream, error_count, bins, overflow_count)
+        none = _abi.GridField()
+        check(_lib().picasso_apic_p2g_update(
+            C.byref(sd.desc), sd.num_particles, particle_field(sd.x), particle_field(m_p),
+            particle_field(c_p), grid_field(m_i), grid_field(mu_i),
+            grid_field(f_i) if f_i is not None else none, C.byref(prm), grid_field(u_i),
+            grid_field(u64_i) if u64_i is not None else none,
+            workspace.data_ptr() if workspace is not None else None,
+            workspace.numel() if workspace is not None else 0, C.byref(ex.desc)),
+            "APIC::p2g_update")
+
+    @staticmethod
     def g2p(u_i, c_p, sd, stream=None, error_count=None, bins=None):
         """APIC::g2p(u_i, c_p, sd): overwrites c_p (4 x ncomp per particle)."""
         ncomp = c_p.shape[2]
@@ -406,12 +433,7 @@ def grid_velocity(mesh_desc, m_i, mu_i, u_i, mass_threshold=1e-12, u64_i=None, s
                                        g64, C.byref(ex.desc)), "grid_velocity")
 
 
-def grid_update(mesh_desc, m_i, mu_i, u_i, dt, gravity=(0.0, 0.0, 0.0), f_i=None,
-                mass_threshold=1e-12, walls=None, wall_width=1, u64_i=None, stream=None,
-                overflow_count=None):
-    """u_i = (mu_i + dt f_i) / m_i + dt g where m_i > threshold (else 0), then
-    wall conditions along non-periodic dimensions: ``walls[d] = (low, high)``
-    with "none", "no_slip" or "free_slip"."""
+def _update_params(dt, gravity, mass_threshold, walls, wall_width):
     kinds = {"none": _abi.WALL_NONE, "no_slip": _abi.WALL_NO_SLIP,
              "free_slip": _abi.WALL_FREE_SLIP}
     prm = _abi.GridUpdateParams()
@@ -422,6 +444,16 @@ def grid_update(mesh_desc, m_i, mu_i, u_i, dt, gravity=(0.0, 0.0, 0.0), f_i=None
             prm.wall[d][side] = kinds[walls[d][side]] if walls else _abi.WALL_NONE
     prm.mass_threshold = float(mass_threshold)
     prm.wall_width = int(wall_width)
+    return prm
+
+
+def grid_update(mesh_desc, m_i, mu_i, u_i, dt, gravity=(0.0, 0.0, 0.0), f_i=None,
+                mass_threshold=1e-12, walls=None, wall_width=1, u64_i=None, stream=None,
+                overflow_count=None):
+    """u_i = (mu_i + dt f_i) / m_i + dt g where m_i > threshold (else 0), then
+    wall conditions along non-periodic dimensions: ``walls[d] = (low, high)``
+    with "none", "no_slip" or "free_slip"."""
+    prm = _update_params(dt, gravity, mass_threshold, walls, wall_width)
     ex = _exec(stream, None, None, overflow_count)
     none = _abi.GridField()
     check(_lib().picasso_grid_update(C.byref(mesh_desc), grid_field(m_i), grid_field(mu_i),
@@ -565,6 +597,14 @@ def spline_records(sd, bins, out=None, attach=True, stream=None):
     if attach:
         bins.attach_records(out)
     return out
+
+
+def p2g_update_workspace(bins):
+    """Bytes of device workspace APIC.p2g_update needs for these bins."""
+    nbytes = C.c_int64()
+    check(_lib().picasso_apic_p2g_update_workspace(C.byref(bins.desc), C.byref(nbytes)),
+          "p2g_update_workspace")
+    return nbytes.value
 
 
 def sort_workspace(sd, tile=(4, 8, 8)):

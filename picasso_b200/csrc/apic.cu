@@ -122,10 +122,11 @@ picasso_status apic_g2p_plain(const MeshP& mp, int order, int stag, int ncomp, b
 }
 
 // Tiled kernels for binned particles (tiled.cu).
+struct FusedUpdate;
 picasso_status apic_p2g_tiled(const MeshP& mp, int order, int ncomp, Form form, int64_t n,
                               const PField& x, const PField& m, const PField& c, const GField& gm,
                               const GField& gmu, const picasso_bins& bins, int* err,
-                              cudaStream_t st, bool* handled);
+                              cudaStream_t st, bool* handled, const FusedUpdate* fu = nullptr);
 picasso_status apic_g2p_tiled(const MeshP& mp, int order, int ncomp, bool f32, int64_t n,
                               const PField& x, const GField& u, const PField& c,
                               const picasso_bins& bins, int* err, const Advect* adv,

@@ -190,6 +190,34 @@ extern "C" picasso_status picasso_grid_velocity(const picasso_mesh* mesh, int32_
     return check_launch();
 }
 
+picasso_status pb::make_grid_update(const picasso_mesh* mesh, const picasso_grid_update_params* prm,
+                                const picasso_grid_field& m_i, const picasso_grid_field& mu_i,
+                                const picasso_grid_field& f_i, GridUpdate* P)
+{
+    if (!mesh || !prm || prm->wall_width < 0) return PICASSO_ERR_INVALID_ARGUMENT;
+    for (int d = 0; d < 3; ++d)
+        for (int s = 0; s < 2; ++s)
+            if (prm->wall[d][s] < PICASSO_WALL_NONE || prm->wall[d][s] > PICASSO_WALL_FREE_SLIP)
+                return PICASSO_ERR_INVALID_ARGUMENT;
+    const bool force = f_i.data != nullptr;
+    P->dt = prm->dt;
+    P->thr = prm->mass_threshold;
+    const bool fixed = m_i.dtype == PICASSO_I64_FIXED;
+    P->inv_m = fixed ? ldexp(1.0, -m_i.fixed_bits) : 1.0;
+    P->inv_mu = fixed ? ldexp(1.0, -mu_i.fixed_bits) : 1.0;
+    P->inv_f = (force && f_i.dtype == PICASSO_I64_FIXED) ? ldexp(1.0, -f_i.fixed_bits) : 1.0;
+    P->force = force;
+    for (int d = 0; d < 3; ++d) {
+        P->g[d] = prm->gravity[d];
+        const bool walls = !mesh->periodic[d];
+        P->wall[d][0] = walls ? prm->wall[d][0] : PICASSO_WALL_NONE;
+        P->wall[d][1] = walls ? prm->wall[d][1] : PICASSO_WALL_NONE;
+        P->lo_wall[d] = mesh->own_begin[d] + prm->wall_width;
+        P->hi_wall[d] = mesh->own_begin[d] + mesh->own_extent[d] - prm->wall_width;
+    }
+    return PICASSO_OK;
+}
+
 extern "C" picasso_status picasso_grid_update(const picasso_mesh* mesh, picasso_grid_field m_i,
                                               picasso_grid_field mu_i, picasso_grid_field f_i,
                                               const picasso_grid_update_params* prm,
@@ -210,21 +238,8 @@ extern "C" picasso_status picasso_grid_update(const picasso_mesh* mesh, picasso_
     if ((st = validate_gfield(u_i, PICASSO_F64, PICASSO_F32))) return st;
     if (u64_i.data && (st = validate_gfield(u64_i, PICASSO_F64))) return st;
     GridUpdate P;
-    P.dt = prm->dt;
-    P.thr = prm->mass_threshold;
+    if ((st = make_grid_update(mesh, prm, m_i, mu_i, f_i, &P))) return st;
     const bool fixed = m_i.dtype == PICASSO_I64_FIXED;
-    P.inv_m = fixed ? ldexp(1.0, -m_i.fixed_bits) : 1.0;
-    P.inv_mu = fixed ? ldexp(1.0, -mu_i.fixed_bits) : 1.0;
-    P.inv_f = (force && f_i.dtype == PICASSO_I64_FIXED) ? ldexp(1.0, -f_i.fixed_bits) : 1.0;
-    P.force = force;
-    for (int d = 0; d < 3; ++d) {
-        P.g[d] = prm->gravity[d];
-        const bool walls = !mesh->periodic[d];
-        P.wall[d][0] = walls ? prm->wall[d][0] : PICASSO_WALL_NONE;
-        P.wall[d][1] = walls ? prm->wall[d][1] : PICASSO_WALL_NONE;
-        P.lo_wall[d] = mesh->own_begin[d] + prm->wall_width;
-        P.hi_wall[d] = mesh->own_begin[d] + mesh->own_extent[d] - prm->wall_width;
-    }
     Box b = owned_box(*mesh);
     GField gm = make_gfield(m_i), gmu = make_gfield(mu_i), gf = make_gfield(f_i);
     GField gu = make_gfield(u_i), gu64 = make_gfield(u64_i);

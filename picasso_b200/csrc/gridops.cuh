@@ -83,19 +83,22 @@ struct GridUpdate {
     bool force;
 };
 
-template <class MT, class FT, class UT>
+// CG: the accumulators are read through L2 only (written by other blocks of
+// the same launch).
+template <class MT, class FT, class UT, bool CG = false>
 __device__ __forceinline__ void update_node(const GridUpdate& P, const GField& gm,
                                             const GField& gmu, const GField& gf, const GField& gu,
                                             const GField& gu64, int i, int j, int k)
 {
-    const MT raw = *gm.ptr<MT>(i, j, k, 0);
+    auto load = [](const MT* a) { return CG ? __ldcg(a) : *a; };
+    const MT raw = load(gm.ptr<MT>(i, j, k, 0));
     count_wrapped_mass(gm, raw);
     const double m = __dmul_rn((double)raw, P.inv_m);
     const bool keep = m > P.thr;
     double u[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        double p = __dmul_rn((double)*gmu.ptr<MT>(i, j, k, c), P.inv_mu);
+        double p = __dmul_rn((double)load(gmu.ptr<MT>(i, j, k, c)), P.inv_mu);
         if (P.force) p = __dadd_rn(p, __dmul_rn(P.dt, __dmul_rn((double)*gf.ptr<FT>(i, j, k, c), P.inv_f)));
         u[c] = keep ? __dadd_rn(__ddiv_rn(p, m), __dmul_rn(P.dt, P.g[c])) : 0.0;
     }
@@ -114,6 +117,12 @@ __device__ __forceinline__ void update_node(const GridUpdate& P, const GField& g
         if (gu64.data) *gu64.ptr<double>(i, j, k, c) = u[c];
     }
 }
+
+// Parameters of the grid update for a mesh, update settings and the grids'
+// types; PICASSO_ERR_INVALID_ARGUMENT for bad settings (grid.cu).
+picasso_status make_grid_update(const picasso_mesh* mesh, const picasso_grid_update_params* prm,
+                                const picasso_grid_field& m_i, const picasso_grid_field& mu_i,
+                                const picasso_grid_field& f_i, GridUpdate* P);
 
 // Position update x += dt v with periodic wrap into the owned box, FP64,
 // rounded step by step as x + (dt * v) (no FMA, so every path that advects

@@ -19,9 +19,9 @@ struct G2PThreads {
     static constexpr int value = ORDER == 3 ? 32 : 64;
 };
 
-template <int ORDER, int LPP, bool REC>
+template <int ORDER, int LPP, bool REC, bool FUSED>
 __global__ void __launch_bounds__(32, (P2GOccupancy<ORDER, LPP>::value))
-p2g_tiled_kernel(P2GArgs A, int64_t n)
+p2g_tiled_kernel(P2GArgs A, FusedUpdate F, int64_t n)
 {
     extern __shared__ __align__(16) float smem[];
     __shared__ int stage_base[kStageLanes];
@@ -32,6 +32,7 @@ p2g_tiled_kernel(P2GArgs A, int64_t n)
     int64_t t, a, b;
     if (!item_range(A.tp, blockIdx.x, t, a, b)) return;
     p2g_item<ORDER, LPP, REC>(A, t, a, b, smem, stage_base);
+    if constexpr (FUSED) fused_update_arrive<ORDER>(A, F, t);
 }
 
 template <int ORDER, bool ADV, bool REC>
@@ -200,6 +201,19 @@ bool make_tilep(const MeshP& mp, int order, const picasso_bins& bins, TileP* tp,
     return bins.tile_offset && bins.tile_items && bins.chunk >= 32;
 }
 
+// The fused update needs every tile (the last one included) to hold at least
+// K - 1 bins along each dimension, so that a node is touched by the items of
+// its own tile and of the previous one only.
+bool fused_update_fits(const TileP& tp, int order)
+{
+    const int K = order + 1;
+    for (int d = 0; d < 3; ++d) {
+        const int last = tp.nb[d] - (tp.nt[d] - 1) * tp.T[d];
+        if (tp.T[d] < K - 1 || last < K - 1) return false;
+    }
+    return true;
+}
+
 int device_smem_optin()
 {
     int dev = 0, v = 0;
@@ -241,13 +255,22 @@ static int64_t item_bound(const TileP& tp, int64_t n)
 }
 
 template <int ORDER, int LPP, bool REC>
-static picasso_status launch_p2g_tiled(const P2GArgs& A, int64_t n, cudaStream_t st)
+static picasso_status launch_p2g_tiled(const P2GArgs& A, const FusedUpdate* fu, int64_t n,
+                                       cudaStream_t st)
 {
     const size_t smem = p2g_warp_bytes(ORDER, LPP, A.tp.P, REC);
-    PB_CUDA_TRY(cudaFuncSetAttribute(p2g_tiled_kernel<ORDER, LPP, REC>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int64_t items = item_bound(A.tp, n);
-    p2g_tiled_kernel<ORDER, LPP, REC><<<(unsigned)(items ? items : 1), 32, smem, st>>>(A, n);
+    if (fu) {
+        PB_CUDA_TRY(cudaFuncSetAttribute(p2g_tiled_kernel<ORDER, LPP, REC, true>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        p2g_tiled_kernel<ORDER, LPP, REC, true>
+            <<<(unsigned)(items ? items : 1), 32, smem, st>>>(A, *fu, n);
+    } else {
+        PB_CUDA_TRY(cudaFuncSetAttribute(p2g_tiled_kernel<ORDER, LPP, REC, false>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        p2g_tiled_kernel<ORDER, LPP, REC, false>
+            <<<(unsigned)(items ? items : 1), 32, smem, st>>>(A, FusedUpdate{}, n);
+    }
     return check_launch();
 }
 
@@ -274,7 +297,7 @@ static const float* bins_records(const picasso_bins& bins)
 picasso_status apic_p2g_tiled(const MeshP& mp, int order, int ncomp, Form form, int64_t n,
                               const PField& x, const PField& m, const PField& c, const GField& gm,
                               const GField& gmu, const picasso_bins& bins, int* err,
-                              cudaStream_t st, bool* handled)
+                              cudaStream_t st, bool* handled, const FusedUpdate* fu)
 {
     *handled = false;
     if (form != Form::F32Fixed || ncomp != 3 || !packed_x(x) || !packed_m(m) || !packed_c(c))
@@ -299,7 +322,8 @@ picasso_status apic_p2g_tiled(const MeshP& mp, int order, int ncomp, Form form, 
     A.err = err;
 #define PB_CASE(O, L)                                                                   \
     if (order == O && lpp == L)                                                         \
-        return rec ? launch_p2g_tiled<O, L, true>(A, n, st) : launch_p2g_tiled<O, L, false>(A, n, st);
+        return rec ? launch_p2g_tiled<O, L, true>(A, fu, n, st)                         \
+                   : launch_p2g_tiled<O, L, false>(A, fu, n, st);
     PB_CASE(1, 1) PB_CASE(1, 2) PB_CASE(1, 4)
     PB_CASE(2, 1) PB_CASE(2, 2) PB_CASE(2, 4)
     PB_CASE(3, 4)
@@ -344,3 +368,88 @@ picasso_status apic_g2p_tiled(const MeshP& mp, int order, int ncomp, bool f32, i
 }
 
 }  // namespace pb
+
+using namespace pb;
+
+// Arrival counters of the fused update: 8 per tile.
+extern "C" picasso_status picasso_apic_p2g_update_workspace(const picasso_bins* bins,
+                                                            int64_t* bytes)
+{
+    if (!bins || !bytes) return PICASSO_ERR_INVALID_ARGUMENT;
+    int64_t nt = 1;
+    for (int d = 0; d < 3; ++d) {
+        if (bins->num_tiles[d] < 1) return PICASSO_ERR_INVALID_ARGUMENT;
+        nt *= bins->num_tiles[d];
+    }
+    *bytes = nt * 8 * (int64_t)sizeof(uint32_t);
+    return PICASSO_OK;
+}
+
+extern "C" picasso_status picasso_apic_p2g_update(
+    const picasso_spline* sd, int64_t num_particles, picasso_particle_field x_p,
+    picasso_particle_field m_p, picasso_particle_field c_p, picasso_grid_field m_i,
+    picasso_grid_field mu_i, picasso_grid_field f_i, const picasso_grid_update_params* prm,
+    picasso_grid_field u_i, picasso_grid_field u64_i, void* workspace, int64_t workspace_bytes,
+    const picasso_exec* exec)
+{
+    MeshP mp;
+    picasso_status st = make_mesh(sd, &mp);
+    if (st) return st;
+    if (num_particles < 0 || !prm) return PICASSO_ERR_INVALID_ARGUMENT;
+    // the separate calls: same results, two passes (validation included)
+    auto separate = [&]() {
+        picasso_status s2 = picasso_apic_p2g(sd, num_particles, 3, x_p, m_p, c_p, m_i, mu_i, exec);
+        if (s2) return s2;
+        return picasso_grid_update(&sd->mesh, m_i, mu_i, f_i, prm, u_i, u64_i, exec);
+    };
+    const picasso_bins* bins = exec ? exec->bins : nullptr;
+    const bool eligible = bins && staggered_dim(sd->location) < 0 && num_particles > 0 &&
+                          m_p.dtype == PICASSO_F32 && m_i.dtype == PICASSO_I64_FIXED &&
+                          mu_i.dtype == PICASSO_I64_FIXED && u_i.dtype == PICASSO_F32 &&
+                          (!f_i.data || f_i.dtype == PICASSO_F64) &&
+                          (!u64_i.data || u64_i.dtype == PICASSO_F64) &&
+                          bins->order == sd->order && bins->location == sd->location;
+    if (!eligible) return separate();
+    if ((st = validate_pfield(num_particles, x_p, PICASSO_F64))) return st;
+    if ((st = validate_pfield(num_particles, m_p, PICASSO_F32))) return st;
+    if ((st = validate_pfield(num_particles, c_p, PICASSO_F32))) return st;
+    if ((st = validate_gfield(m_i, PICASSO_I64_FIXED))) return st;
+    if ((st = validate_gfield(mu_i, PICASSO_I64_FIXED))) return st;
+    if ((st = validate_gfield(u_i, PICASSO_F32))) return st;
+    if (f_i.data && (st = validate_gfield(f_i, PICASSO_F64))) return st;
+    if (u64_i.data && (st = validate_gfield(u64_i, PICASSO_F64))) return st;
+    TileP tp;
+    if (!make_tilep(mp, sd->order, *bins, &tp)) return PICASSO_ERR_INVALID_ARGUMENT;
+    int64_t need = 0;
+    if ((st = picasso_apic_p2g_update_workspace(bins, &need))) return st;
+    if (!fused_update_fits(tp, sd->order)) return separate();
+    if (!workspace || workspace_bytes < need || reinterpret_cast<uintptr_t>(workspace) % 4)
+        return PICASSO_ERR_INVALID_ARGUMENT;
+    FusedUpdate F;
+    if ((st = make_grid_update(&sd->mesh, prm, m_i, mu_i, f_i, &F.P))) return st;
+    F.gf = make_gfield(f_i);
+    F.gu = make_gfield(u_i);
+    F.gu64 = make_gfield(u64_i);
+    F.count = static_cast<uint32_t*>(workspace);
+    cudaStream_t s = stream_of(exec);
+    PB_CUDA_TRY(cudaMemsetAsync(workspace, 0, (size_t)need, s));
+    // nodes of regions that no work item touches get the update of an
+    // empty node, 0
+    {
+        const unsigned blocks = grid_for(tp.ntiles * 8, 256, 148LL * 16);
+        if (sd->order == 1) zero_untouched_regions_kernel<1><<<blocks, 256, 0, s>>>(mp, tp, F);
+        else if (sd->order == 2) zero_untouched_regions_kernel<2><<<blocks, 256, 0, s>>>(mp, tp, F);
+        else zero_untouched_regions_kernel<3><<<blocks, 256, 0, s>>>(mp, tp, F);
+        if ((st = check_launch())) return st;
+    }
+    const PField x = make_pfield(x_p), m = make_pfield(m_p), c = make_pfield(c_p);
+    GField gm = make_gfield(m_i), gmu = make_gfield(mu_i);
+    gm.overflow = gmu.overflow = exec->overflow_count;
+    bool handled = false;
+    st = apic_p2g_tiled(mp, sd->order, 3, Form::F32Fixed, num_particles, x, m, c, gm, gmu, *bins,
+                        exec->error_count, s, &handled, &F);
+    if (st || handled) return st;
+    // the tiled kernel does not take these particles (layout, tile size):
+    // the fill of u above is overwritten by the separate update
+    return separate();
+}

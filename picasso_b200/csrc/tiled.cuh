@@ -814,6 +814,167 @@ __device__ void p2g_item(const P2GArgs& A, int64_t t, int64_t a, int64_t b, floa
 }
 
 // ---------------------------------------------------------------------------
+// P2G with the grid update in its flush
+// ---------------------------------------------------------------------------
+// A node's value is final once every work item that can touch it has added
+// its tile box.  Every node belongs to the tile of the bin with its index
+// (for a non-periodic mesh the last tile along a dimension also takes the
+// K - 1 nodes past the last bin), and a tile's nodes form 8 regions by
+// whether each local index is below K - 1: those nodes are also touched by
+// the items of the previous tile along that dimension, the others only by
+// the tile's own items (tiles of at least K - 1 bins).  An item that has
+// flushed counts its arrival at every region it can touch (27: the tile and
+// its successors along each dimension, their low parts); the item whose
+// arrival completes a region's count (the items of the up to 8 tiles that
+// touch it) converts the region's nodes with the grid update.  The
+// accumulators are exact integer sums, so the conversion sees the same
+// values as a separate update pass after P2G: results are bit-identical.
+struct FusedUpdate {
+    GridUpdate P;
+    GField gf, gu, gu64;  // force (optional, FP64), velocity, FP64 velocity (optional)
+    uint32_t* count;      // 8 arrival counters per tile, zero at launch
+};
+
+// Local node range [lo, hi) of the region part `low` of tile q along d.
+__device__ __forceinline__ void region_range(const MeshP& mp, const TileP& tp, int d, int q,
+                                             int low, int K, int& lo, int& hi)
+{
+    const int teff = min(tp.T[d], tp.nb[d] - q * tp.T[d]);
+    if (low) {
+        lo = 0;
+        hi = K - 1;
+    } else {
+        lo = K - 1;
+        hi = teff + ((!mp.periodic[d] && q == tp.nt[d] - 1) ? K - 1 : 0);
+    }
+}
+
+__device__ __forceinline__ uint32_t tile_items_of(const TileP& tp, int64_t s)
+{
+    return __ldg(tp.items + s + 1) - __ldg(tp.items + s);
+}
+
+// Items of the tiles that touch region `reg` of tile (q0, q1, q2).
+__device__ __forceinline__ uint32_t region_items(const MeshP& mp, const TileP& tp, const int q[3],
+                                                 int reg)
+{
+    uint32_t expected = 0;
+    for (int mm = 0; mm < 8; ++mm) {
+        if (mm & ~reg) continue;
+        int pp[3];
+        bool ok = true;
+        for (int d = 0; d < 3; ++d) {
+            pp[d] = q[d] - ((mm >> d) & 1);
+            if (pp[d] < 0) {
+                if (mp.periodic[d]) pp[d] += tp.nt[d];
+                else ok = false;
+            }
+        }
+        if (ok) expected += tile_items_of(tp, ((int64_t)pp[0] * tp.nt[1] + pp[1]) * tp.nt[2] + pp[2]);
+    }
+    return expected;
+}
+
+// Global node of local index g[d] in tile q along d.
+__device__ __forceinline__ void region_node(const MeshP& mp, const TileP& tp, const int q[3],
+                                            int g[3])
+{
+    for (int d = 0; d < 3; ++d) {
+        g[d] += q[d] * tp.T[d];
+        if (mp.periodic[d]) g[d] += mp.own_lo[d];
+    }
+}
+
+// Called by the whole warp after p2g_item(A, t, ...) has flushed its box.
+template <int ORDER>
+__device__ void fused_update_arrive(const P2GArgs& A, const FusedUpdate& F, int64_t t)
+{
+    constexpr int K = SplineTraits<ORDER>::K;
+    const MeshP& mp = A.mp;
+    const TileP& tp = A.tp;
+    const int lane = threadIdx.x & 31;
+    __threadfence();  // this lane's reductions are visible before its item counts
+    __syncwarp();
+    const int q[3] = {(int)(t / ((int64_t)tp.nt[1] * tp.nt[2])),
+                      (int)((t / tp.nt[2]) % tp.nt[1]), (int)(t % tp.nt[2])};
+    bool last = false;
+    int64_t tt = 0;
+    int reg = 0;
+    if (lane < 27) {
+        // per dimension: 0 = this tile, high part; 1 = this tile, low part;
+        // 2 = the next tile, low part
+        const int o[3] = {lane / 9, (lane / 3) % 3, lane % 3};
+        int qq[3];
+        bool exists = true;
+        for (int d = 0; d < 3; ++d) {
+            qq[d] = q[d] + (o[d] == 2);
+            if (qq[d] >= tp.nt[d]) {
+                if (mp.periodic[d]) qq[d] = 0;
+                else exists = false;
+            }
+            reg |= (o[d] >= 1) << d;
+        }
+        if (exists) {
+            tt = ((int64_t)qq[0] * tp.nt[1] + qq[1]) * tp.nt[2] + qq[2];
+            // the items of the tiles that touch the region: qq and, along
+            // the region's low dimensions, the previous tile
+            const uint32_t expected = region_items(mp, tp, qq, reg);
+            const uint32_t old = atomicAdd(F.count + tt * 8 + reg, 1u);
+            last = old + 1 == expected;
+        }
+    }
+    unsigned lm = __ballot_sync(kFull, last);
+    while (lm) {
+        const int src = __ffs(lm) - 1;
+        lm &= lm - 1;
+        const int64_t ct = __shfl_sync(kFull, tt, src);
+        const int cr = __shfl_sync(kFull, reg, src);
+        __threadfence();  // every arrival counted: their reductions are visible
+        const int cq[3] = {(int)(ct / ((int64_t)tp.nt[1] * tp.nt[2])),
+                           (int)((ct / tp.nt[2]) % tp.nt[1]), (int)(ct % tp.nt[2])};
+        int lo[3], hi[3];
+        for (int d = 0; d < 3; ++d) region_range(mp, tp, d, cq[d], (cr >> d) & 1, K, lo[d], hi[d]);
+        const int n1 = hi[1] - lo[1], n2 = hi[2] - lo[2];
+        const int total = (hi[0] - lo[0]) * n1 * n2;
+        for (int e = lane; e < total; e += 32) {
+            int g[3] = {lo[0] + e / (n1 * n2), lo[1] + (e / n2) % n1, lo[2] + e % n2};
+            region_node(mp, tp, cq, g);
+            update_node<long long, double, float, true>(F.P, A.gm, A.gmu, F.gf, F.gu, F.gu64,
+                                                        g[0], g[1], g[2]);
+        }
+    }
+}
+
+// Regions no work item touches are converted by no item: one thread per
+// (tile, region) writes them the update of an empty node, 0.
+template <int ORDER>
+__global__ void zero_untouched_regions_kernel(MeshP mp, TileP tp, FusedUpdate F)
+{
+    constexpr int K = SplineTraits<ORDER>::K;
+    const int64_t total = tp.ntiles * 8;
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < total;
+         r += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t t = r / 8;
+        const int reg = (int)(r % 8);
+        const int q[3] = {(int)(t / ((int64_t)tp.nt[1] * tp.nt[2])),
+                          (int)((t / tp.nt[2]) % tp.nt[1]), (int)(t % tp.nt[2])};
+        if (region_items(mp, tp, q, reg) != 0) continue;
+        int lo[3], hi[3];
+        for (int d = 0; d < 3; ++d) region_range(mp, tp, d, q[d], (reg >> d) & 1, K, lo[d], hi[d]);
+        for (int i = lo[0]; i < hi[0]; ++i)
+            for (int j = lo[1]; j < hi[1]; ++j)
+                for (int k = lo[2]; k < hi[2]; ++k) {
+                    int g[3] = {i, j, k};
+                    region_node(mp, tp, q, g);
+                    for (int c = 0; c < 3; ++c) {
+                        *F.gu.ptr<float>(g[0], g[1], g[2], c) = 0.f;
+                        if (F.gu64.data) *F.gu64.ptr<double>(g[0], g[1], g[2], c) = 0.0;
+                    }
+                }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // G2P
 // ---------------------------------------------------------------------------
 // One G2P work item by NTHR threads (a warp or a CTA) sharing `tile`
@@ -983,6 +1144,7 @@ __device__ void g2p_item(const G2PArgs& A, int64_t t, int64_t a, int64_t b, floa
 }
 
 // host helpers (tiled.cu)
+bool fused_update_fits(const TileP& tp, int order);
 bool make_tilep(const MeshP& mp, int order, const picasso_bins& bins, TileP* tp, int lpp = 0);
 int device_smem_optin();
 bool packed_x(const PField& x);

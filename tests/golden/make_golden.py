@@ -11,7 +11,8 @@ width, particle mass/position/cell, time step, tolerance).
 It only runs where the reference tree is present; the JSON it produced is
 committed and is what the tests read.
 
-Usage:  python tests/golden/make_golden.py [REFERENCE_ROOT]
+Usage:  python tests/golden/make_golden.py REFERENCE_ROOT
+        (or PICASSO_REFERENCE_ROOT=... python tests/golden/make_golden.py)
 """
 
 import json
@@ -65,7 +66,10 @@ def parse_fixture(text):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PICASSO_REFERENCE_ROOT")
+    if not ref:
+        sys.exit("usage: make_golden.py <Picasso source tree> "
+                 "(or set PICASSO_REFERENCE_ROOT)")
     ut = os.path.join(ref, "unit_test")
     out = {"source": "reference unit_test/tstAPIC.hpp and unit_test/tstPolyPIC.hpp "
                      "(Mathematica-generated known answers)"}
