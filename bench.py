@@ -52,8 +52,9 @@ def parse():
     ap.add_argument("--p2g-lanes", type=int, default=0,
                     help="lanes per particle of the tiled P2G (0 = library choice)")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 plain leg")
-    ap.add_argument("--no-fuse", action="store_true",
-                    help="grid velocity as a separate pass instead of inside the P2G launch")
+    ap.add_argument("--fuse", action="store_true",
+                    help="grid velocity inside the P2G launch (APIC.p2g_update) instead of "
+                         "its own pass")
     ap.add_argument("--no-records", action="store_true",
                     help="tiled kernels read the positions instead of spline records")
     ap.add_argument("--batch-leg-instances", type=int, default=96,
@@ -523,7 +524,9 @@ def run_ours(args):
 
     out = {}
     # FP32 precision form (headline)
-    fused = bins is not None and not args.no_fuse
+    # the grid velocity as its own pass (measured faster than inside the P2G
+    # launch, which is reported beside it); --fuse puts it inside
+    fused = bins is not None and args.fuse
     s32 = Step("fp32", mesh, x, m32, c32.clone(), bins, stream, fused=fused)
     clk.start()
     ms32, per32 = time_form(s32, args.steps, args.warmup, dist)
@@ -544,13 +547,13 @@ def run_ours(args):
                           else None}
         del sx
         bins.attach_records(rec_keep)
-    unfused = None
-    if fused:
-        # the same step with the grid velocity as a separate pass
-        sf_ = Step("fp32", mesh, x, m32, c32.clone(), bins, stream, fused=False)
+    other = None
+    if bins is not None:
+        # the same step with the grid velocity in the other place
+        sf_ = Step("fp32", mesh, x, m32, c32.clone(), bins, stream, fused=not fused)
         msf, perf = time_form(sf_, args.steps, args.warmup, dist)
-        unfused = {"ms_per_step": msf, "particles_per_s": world * n / (msf * 1e-3),
-                   "kernels_ms": perf}
+        other = {"ms_per_step": msf, "particles_per_s": world * n / (msf * 1e-3),
+                 "kernels_ms": perf}
         del sf_
     # FP64 plain form: on the generation-order particles (no sort, as the
     # reference runs) and on the cell-sorted ones
@@ -632,8 +635,8 @@ def run_ours(args):
             "clocks": clocks}
     if from_positions:
         line["fp32_from_positions"] = from_positions
-    if unfused:
-        line["fp32_separate_velocity_pass"] = unfused
+    if other:
+        line["fp32_separate_velocity_pass" if fused else "fp32_velocity_fused_into_p2g"] = other
     line["step"] = ("fill (memset), P2G with the grid velocity update fused into its flush, G2P"
                     if fused else "fill (memset), P2G, grid velocity, G2P")
     if "fp64" in out:
@@ -731,8 +734,7 @@ def run_advect(args, peak):
     res = {"workload": "cubic APIC, %d^3 periodic, 8 ppc uniform, dt = 0.1 dx, per step: "
                        "cell re-sort (from the keys the previous G2P emitted) + permute (FP32 "
                        "form: + spline records of the permuted particles), fill, P2G, "
-                       "velocity (FP32 form: inside the P2G launch), G2P + advection + sort "
-                       "keys" % g,
+                       "velocity, G2P + advection + sort keys" % g,
            "steps": args.adv_steps, "tile": list(args.adv_tile)}
     names = ["sort", "permute", "fill", "p2g", "velocity", "g2p_advect"]
     for form in ("fp64", "fp32"):
@@ -782,7 +784,7 @@ def run_advect(args, peak):
             mark(2)
             pb.grid_fill(desc, fill, 0.0, ncomp=4)
             mark(3)
-            if f32:
+            if f32 and args.fuse:
                 if "ws" not in fws:
                     fws["ws"] = torch.empty(pb.p2g_update_workspace(bins), dtype=torch.uint8,
                                             device="cuda")
@@ -818,8 +820,8 @@ def run_advect(args, peak):
         px = 16 if f32 else 24  # FP32 form: P2G reads the spline records
         kb = {"permute": n * (2 * (24 + sf + 12 * sf) + 3 * 4 + (24 + 16 if f32 else 0)),
               "fill": nodes * 32,
-              "p2g": n * (px + 13 * sf) + nodes * (32 + (3 * sf if f32 else 0)),
-              "velocity": 0 if f32 else nodes * (32 + 3 * sf),
+              "p2g": n * (px + 13 * sf) + nodes * (32 + (3 * sf if f32 and args.fuse else 0)),
+              "velocity": 0 if f32 and args.fuse else nodes * (32 + 3 * sf),
               "g2p_advect": n * (24 + 24 + 12 * sf + 4) + nodes * 3 * sf}
         step_bytes = sum(kb.values())
         res[form] = {"ms_per_step": ms, "particles_per_s": n / (ms * 1e-3),

@@ -126,11 +126,12 @@ struct FusedUpdate;
 picasso_status apic_p2g_tiled(const MeshP& mp, int order, int ncomp, Form form, int64_t n,
                               const PField& x, const PField& m, const PField& c, const GField& gm,
                               const GField& gmu, const picasso_bins& bins, int* err,
-                              cudaStream_t st, bool* handled, const FusedUpdate* fu = nullptr);
+                              cudaStream_t st, bool* handled, const FusedUpdate* fu = nullptr,
+                              int stag = -1);
 picasso_status apic_g2p_tiled(const MeshP& mp, int order, int ncomp, bool f32, int64_t n,
                               const PField& x, const GField& u, const PField& c,
                               const picasso_bins& bins, int* err, const Advect* adv,
-                              cudaStream_t st, bool* handled);
+                              cudaStream_t st, bool* handled, int stag = -1);
 
 }  // namespace pb
 
@@ -169,11 +170,9 @@ extern "C" picasso_status picasso_apic_p2g(const picasso_spline* sd, int64_t num
         if (exec->bins->order != sd->order || exec->bins->location != sd->location)
             return PICASSO_ERR_INVALID_ARGUMENT;
         bool handled = false;
-        if (stag < 0) {
-            st = apic_p2g_tiled(mp, sd->order, ncomp, form, num_particles, x, m, c, gm, gmu,
-                                *exec->bins, err, s, &handled);
-            if (st || handled) return st;
-        }
+        st = apic_p2g_tiled(mp, sd->order, ncomp, form, num_particles, x, m, c, gm, gmu,
+                            *exec->bins, err, s, &handled, nullptr, stag);
+        if (st || handled) return st;
     }
     return apic_p2g_plain(mp, sd->order, stag, ncomp, form, num_particles, x, m, c, gm, gmu,
                           err, s);
@@ -222,11 +221,9 @@ static picasso_status apic_g2p_entry(const picasso_spline* sd, int64_t num_parti
         if (exec->bins->order != sd->order || exec->bins->location != sd->location)
             return PICASSO_ERR_INVALID_ARGUMENT;
         bool handled = false;
-        if (stag < 0) {
-            st = apic_g2p_tiled(mp, sd->order, ncomp, f32, num_particles, x, u, c, *exec->bins,
-                                err, ap, s, &handled);
-            if (st || handled) return st;
-        }
+        st = apic_g2p_tiled(mp, sd->order, ncomp, f32, num_particles, x, u, c, *exec->bins, err,
+                            ap, s, &handled, stag);
+        if (st || handled) return st;
     }
     return apic_g2p_plain(mp, sd->order, stag, ncomp, f32, num_particles, x, u, c, err, ap, s);
 }

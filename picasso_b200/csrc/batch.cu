@@ -503,12 +503,14 @@ picasso_status make_instance(const picasso_batch_instance& in, bool f32, BInst* 
     I->p2g.scale_m = f32 ? ldexpf(1.f, in.m_i.fixed_bits) : 0.f;
     I->p2g.scale_mu = f32 ? ldexpf(1.f, in.mu_i.fixed_bits) : 0.f;
     I->p2g.err = in.error_count;
+    I->p2g.stag = -1;
     I->g2p.mp = mp;
     I->g2p.tp = tp;
     I->g2p.x = I->p2g.x;
     I->g2p.u = make_gfield(in.u_i);
     I->g2p.c = reinterpret_cast<float*>(in.c_p.data);
     I->g2p.err = in.error_count;
+    I->g2p.stag = -1;
     I->x = x;
     I->m = m;
     I->c = c;

@@ -19,7 +19,7 @@ struct G2PThreads {
     static constexpr int value = ORDER == 3 ? 32 : 64;
 };
 
-template <int ORDER, int LPP, bool REC, bool FUSED>
+template <int ORDER, int LPP, bool REC, bool FUSED, bool STAG>
 __global__ void __launch_bounds__(32, (P2GOccupancy<ORDER, LPP>::value))
 p2g_tiled_kernel(P2GArgs A, FusedUpdate F, int64_t n)
 {
@@ -31,11 +31,11 @@ p2g_tiled_kernel(P2GArgs A, FusedUpdate F, int64_t n)
     }
     int64_t t, a, b;
     if (!item_range(A.tp, blockIdx.x, t, a, b)) return;
-    p2g_item<ORDER, LPP, REC>(A, t, a, b, smem, stage_base);
+    p2g_item<ORDER, LPP, REC, STAG>(A, t, a, b, smem, stage_base);
     if constexpr (FUSED) fused_update_arrive<ORDER>(A, F, t);
 }
 
-template <int ORDER, bool ADV, bool REC>
+template <int ORDER, bool ADV, bool REC, bool STAG>
 __global__ void __launch_bounds__(G2PThreads<ORDER>::value) g2p_tiled_kernel(G2PArgs A, int64_t n)
 {
     extern __shared__ __align__(16) float smem[];
@@ -45,7 +45,7 @@ __global__ void __launch_bounds__(G2PThreads<ORDER>::value) g2p_tiled_kernel(G2P
     }
     int64_t t, a, b;
     if (!item_range(A.tp, blockIdx.x, t, a, b)) return;  // CTA-uniform
-    g2p_item<ORDER, G2PThreads<ORDER>::value, ADV, REC>(A, t, a, b,
+    g2p_item<ORDER, G2PThreads<ORDER>::value, ADV, REC, STAG>(A, t, a, b,
                                                        reinterpret_cast<float4*>(smem),
                                                        threadIdx.x);
 }
@@ -93,7 +93,10 @@ static void search_strides(const StrideKey& key, int* SJ, int* SI, int* P)
                         if (v >= SV || nn >= NL) continue;
                         const int a = nn / (K * K), b = (nn / K) % K, c = nn % K;
                         const int off = f * pp + a * si + b * sj + c;
-                        const unsigned bit = 1u << (off & 31);
+                        // 8-byte tile words: a half warp per bank cycle
+                        const unsigned bit = kTileWords == 2
+                                                 ? (1u << ((off & 15) + 16 * (lane >> 4)))
+                                                 : (1u << (off & 31));
                         if (!(banks & bit)) ++distinct;
                         banks |= bit;
                     }
@@ -105,12 +108,14 @@ static void search_strides(const StrideKey& key, int* SJ, int* SI, int* P)
                         if (v >= PV) continue;
                         const int ij = v % ROWS;
                         const int off = (v / ROWS) * pp + (ij / K) * si + (ij % K) * sj;
-                        const unsigned bit = 1u << (off & 31);
+                        const unsigned bit = kTileWords == 2
+                                                 ? (1u << ((off & 15) + 16 * (lane >> 4)))
+                                                 : (1u << (off & 31));
                         if (!(banks & bit)) ++distinct;
                         banks |= bit;
                     }
                 }
-                const long size = 4L * pp;
+                const long size = 4L * pp * kTileWords;
                 if (distinct > best || (distinct == best && size < best_size)) {
                     best = distinct;
                     best_size = size;
@@ -157,16 +162,17 @@ static_assert(P2GCfg<3, 4>::ISPLIT && !P2GCfg<2, 4>::ISPLIT && !P2GCfg<1, 4>::IS
 
 int default_lpp(int order) { return order == 3 ? 4 : 1; }
 
-// Orders 1 and 2 take 1, 2 or 4 lanes per particle; order 3 (4 x 64
-// accumulators) takes 4.
-bool valid_lpp(int order, int lpp)
+// Orders 1 and 2 take 1, 2 or 4 lanes per particle (staggered locations, with
+// two grid fields: 1 or 2); order 3 (4 x 64 accumulators) takes 4.
+bool valid_lpp(int order, int lpp, bool stag)
 {
     if (order == 3) return lpp == 4;
-    return lpp == 1 || lpp == 2 || lpp == 4;
+    return lpp == 1 || lpp == 2 || (lpp == 4 && !stag);
 }
 
-// Tile geometry for the bins; lpp > 0 also picks the P2G tile strides.
-bool make_tilep(const MeshP& mp, int order, const picasso_bins& bins, TileP* tp, int lpp)
+// Tile geometry for the bins; lpp > 0 also picks the P2G tile strides for nf
+// grid fields.
+bool make_tilep(const MeshP& mp, int order, const picasso_bins& bins, TileP* tp, int lpp, int nf)
 {
     const int K = order + 1;
     int64_t nt = 1;
@@ -188,7 +194,7 @@ bool make_tilep(const MeshP& mp, int order, const picasso_bins& bins, TileP* tp,
     if (lpp > 0) {
         // the accumulator split of p2g_item (P2GCfg::ISPLIT, F)
         const int split = order == 3 && lpp == 4;
-        choose_strides(tp->NT, K, split ? 4 : 4 / lpp, split, &tp->SJ, &tp->SI, &tp->P);
+        choose_strides(tp->NT, K, split ? nf : nf / lpp, split, &tp->SJ, &tp->SI, &tp->P);
     } else {
         tp->SJ = tp->NT[2];
         tp->SI = tp->NT[1] * tp->NT[2];
@@ -236,15 +242,17 @@ bool packed_c(const PField& c)
            (reinterpret_cast<uintptr_t>(c.data) % 16) == 0;
 }
 
-size_t p2g_warp_bytes(int order, int lpp, int P, bool rec)
+size_t p2g_warp_bytes(int order, int lpp, int P, bool rec, bool stag)
 {
-#define PB_CASE(O, L)                                                                   \
-    if (order == O && lpp == L)                                                         \
-        return sizeof(float) * (size_t)(rec ? p2g_warp_floats<O, L, true>(P)            \
-                                            : p2g_warp_floats<O, L, false>(P));
-    PB_CASE(1, 1) PB_CASE(1, 2) PB_CASE(1, 4)
-    PB_CASE(2, 1) PB_CASE(2, 2) PB_CASE(2, 4)
-    PB_CASE(3, 4)
+#define PB_CASE(O, L, S)                                                                \
+    if (order == O && lpp == L && stag == S)                                            \
+        return sizeof(float) * (size_t)(rec ? p2g_warp_floats<O, L, true, S>(P)         \
+                                            : p2g_warp_floats<O, L, false, S>(P));
+    PB_CASE(1, 1, false) PB_CASE(1, 2, false) PB_CASE(1, 4, false)
+    PB_CASE(2, 1, false) PB_CASE(2, 2, false) PB_CASE(2, 4, false)
+    PB_CASE(3, 4, false)
+    PB_CASE(1, 1, true) PB_CASE(1, 2, true) PB_CASE(2, 1, true) PB_CASE(2, 2, true)
+    PB_CASE(3, 4, true)
 #undef PB_CASE
     return 0;
 }
@@ -254,34 +262,39 @@ static int64_t item_bound(const TileP& tp, int64_t n)
     return tp.ntiles + (n + tp.chunk - 1) / tp.chunk;
 }
 
-template <int ORDER, int LPP, bool REC>
+template <int ORDER, int LPP, bool REC, bool STAG>
 static picasso_status launch_p2g_tiled(const P2GArgs& A, const FusedUpdate* fu, int64_t n,
                                        cudaStream_t st)
 {
-    const size_t smem = p2g_warp_bytes(ORDER, LPP, A.tp.P, REC);
+    const size_t smem = p2g_warp_bytes(ORDER, LPP, A.tp.P, REC, STAG);
     const int64_t items = item_bound(A.tp, n);
-    if (fu) {
-        PB_CUDA_TRY(cudaFuncSetAttribute(p2g_tiled_kernel<ORDER, LPP, REC, true>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        p2g_tiled_kernel<ORDER, LPP, REC, true>
-            <<<(unsigned)(items ? items : 1), 32, smem, st>>>(A, *fu, n);
-    } else {
-        PB_CUDA_TRY(cudaFuncSetAttribute(p2g_tiled_kernel<ORDER, LPP, REC, false>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        p2g_tiled_kernel<ORDER, LPP, REC, false>
-            <<<(unsigned)(items ? items : 1), 32, smem, st>>>(A, FusedUpdate{}, n);
+    if constexpr (!STAG) {
+        if (fu) {
+            PB_CUDA_TRY(cudaFuncSetAttribute(p2g_tiled_kernel<ORDER, LPP, REC, true, false>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem));
+            p2g_tiled_kernel<ORDER, LPP, REC, true, false>
+                <<<(unsigned)(items ? items : 1), 32, smem, st>>>(A, *fu, n);
+            return check_launch();
+        }
+    } else if (fu) {
+        return PICASSO_ERR_UNSUPPORTED;  // the fused update is collocated
     }
+    PB_CUDA_TRY(cudaFuncSetAttribute(p2g_tiled_kernel<ORDER, LPP, REC, false, STAG>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    p2g_tiled_kernel<ORDER, LPP, REC, false, STAG>
+        <<<(unsigned)(items ? items : 1), 32, smem, st>>>(A, FusedUpdate{}, n);
     return check_launch();
 }
 
-template <int ORDER, bool ADV, bool REC>
+template <int ORDER, bool ADV, bool REC, bool STAG>
 static picasso_status launch_g2p_tiled(const G2PArgs& A, int64_t n, cudaStream_t st)
 {
     const size_t smem = sizeof(float4) * (size_t)A.tp.nodes;
-    PB_CUDA_TRY(cudaFuncSetAttribute(g2p_tiled_kernel<ORDER, ADV, REC>,
+    PB_CUDA_TRY(cudaFuncSetAttribute(g2p_tiled_kernel<ORDER, ADV, REC, STAG>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int64_t items = item_bound(A.tp, n);
-    g2p_tiled_kernel<ORDER, ADV, REC>
+    g2p_tiled_kernel<ORDER, ADV, REC, STAG>
         <<<(unsigned)(items ? items : 1), G2PThreads<ORDER>::value, smem, st>>>(A, n);
     return check_launch();
 }
@@ -294,24 +307,28 @@ static const float* bins_records(const picasso_bins& bins)
     return (r && r % 16 == 0) ? static_cast<const float*>(bins.records) : nullptr;
 }
 
+// stag: the entity's dimension of a staggered location (its grid fields are
+// the mass and one momentum component: c_p column stag), else -1.
 picasso_status apic_p2g_tiled(const MeshP& mp, int order, int ncomp, Form form, int64_t n,
                               const PField& x, const PField& m, const PField& c, const GField& gm,
                               const GField& gmu, const picasso_bins& bins, int* err,
-                              cudaStream_t st, bool* handled, const FusedUpdate* fu)
+                              cudaStream_t st, bool* handled, const FusedUpdate* fu, int stag)
 {
     *handled = false;
     if (form != Form::F32Fixed || ncomp != 3 || !packed_x(x) || !packed_m(m) || !packed_c(c))
         return PICASSO_OK;
+    const bool sg = stag >= 0;
     const int lpp = bins.p2g_lanes ? bins.p2g_lanes : default_lpp(order);
-    if (!valid_lpp(order, lpp)) return PICASSO_ERR_INVALID_ARGUMENT;
+    if (!valid_lpp(order, lpp, sg)) return PICASSO_ERR_INVALID_ARGUMENT;
     P2GArgs A;
-    if (!make_tilep(mp, order, bins, &A.tp, lpp)) return PICASSO_ERR_INVALID_ARGUMENT;
+    if (!make_tilep(mp, order, bins, &A.tp, lpp, sg ? 2 : 4)) return PICASSO_ERR_INVALID_ARGUMENT;
     A.rec = bins_records(bins);
     const bool rec = A.rec != nullptr;
-    const size_t smem = p2g_warp_bytes(order, lpp, A.tp.P, rec);
+    const size_t smem = p2g_warp_bytes(order, lpp, A.tp.P, rec, sg);
     if ((int64_t)smem > device_smem_optin()) return PICASSO_OK;  // tile too large: plain path
     *handled = true;
     A.mp = mp;
+    A.stag = stag;
     A.x = reinterpret_cast<const double*>(x.data);
     A.m = reinterpret_cast<const float*>(m.data);
     A.c = reinterpret_cast<const float*>(c.data);
@@ -320,30 +337,47 @@ picasso_status apic_p2g_tiled(const MeshP& mp, int order, int ncomp, Form form, 
     A.scale_m = ldexpf(1.f, gm.fixed_bits);
     A.scale_mu = ldexpf(1.f, gmu.fixed_bits);
     A.err = err;
-#define PB_CASE(O, L)                                                                   \
-    if (order == O && lpp == L)                                                         \
-        return rec ? launch_p2g_tiled<O, L, true>(A, fu, n, st)                         \
-                   : launch_p2g_tiled<O, L, false>(A, fu, n, st);
-    PB_CASE(1, 1) PB_CASE(1, 2) PB_CASE(1, 4)
-    PB_CASE(2, 1) PB_CASE(2, 2) PB_CASE(2, 4)
-    PB_CASE(3, 4)
+#define PB_CASE(O, L, S)                                                                \
+    if (order == O && lpp == L && sg == S)                                              \
+        return rec ? launch_p2g_tiled<O, L, true, S>(A, fu, n, st)                      \
+                   : launch_p2g_tiled<O, L, false, S>(A, fu, n, st);
+    PB_CASE(1, 1, false) PB_CASE(1, 2, false) PB_CASE(1, 4, false)
+    PB_CASE(2, 1, false) PB_CASE(2, 2, false) PB_CASE(2, 4, false)
+    PB_CASE(3, 4, false)
+    PB_CASE(1, 1, true) PB_CASE(1, 2, true) PB_CASE(2, 1, true) PB_CASE(2, 2, true)
+    PB_CASE(3, 4, true)
 #undef PB_CASE
     return PICASSO_ERR_INVALID_ARGUMENT;
+}
+
+template <int ORDER>
+static picasso_status launch_g2p_order(const G2PArgs& A, int64_t n, cudaStream_t st, bool adv,
+                                       bool stag)
+{
+    if (adv) return launch_g2p_tiled<ORDER, true, false, false>(A, n, st);
+    if (stag) {
+        if (A.rec) return launch_g2p_tiled<ORDER, false, true, true>(A, n, st);
+        return launch_g2p_tiled<ORDER, false, false, true>(A, n, st);
+    }
+    if (A.rec) return launch_g2p_tiled<ORDER, false, true, false>(A, n, st);
+    return launch_g2p_tiled<ORDER, false, false, false>(A, n, st);
 }
 
 picasso_status apic_g2p_tiled(const MeshP& mp, int order, int ncomp, bool f32, int64_t n,
                               const PField& x, const GField& u, const PField& c,
                               const picasso_bins& bins, int* err, const Advect* adv,
-                              cudaStream_t st, bool* handled)
+                              cudaStream_t st, bool* handled, int stag)
 {
     *handled = false;
     if (!f32 || ncomp != 3 || !packed_x(x) || !packed_c(c)) return PICASSO_OK;
+    if (adv && stag >= 0) return PICASSO_OK;
     G2PArgs A;
     if (!make_tilep(mp, order, bins, &A.tp)) return PICASSO_ERR_INVALID_ARGUMENT;
     const size_t smem = sizeof(float4) * (size_t)A.tp.nodes;
     if ((int64_t)smem > device_smem_optin()) return PICASSO_OK;
     *handled = true;
     A.mp = mp;
+    A.stag = stag;
     A.x = reinterpret_cast<const double*>(x.data);
     A.u = u;
     A.c = reinterpret_cast<float*>(c.data);
@@ -352,19 +386,9 @@ picasso_status apic_g2p_tiled(const MeshP& mp, int order, int ncomp, bool f32, i
     A.adv = adv ? *adv : Advect{};
     // the advection needs the positions; without it the records replace them
     A.rec = adv ? nullptr : reinterpret_cast<const float4*>(bins_records(bins));
-    if (adv) {
-        if (order == 1) return launch_g2p_tiled<1, true, false>(A, n, st);
-        if (order == 2) return launch_g2p_tiled<2, true, false>(A, n, st);
-        return launch_g2p_tiled<3, true, false>(A, n, st);
-    }
-    if (A.rec) {
-        if (order == 1) return launch_g2p_tiled<1, false, true>(A, n, st);
-        if (order == 2) return launch_g2p_tiled<2, false, true>(A, n, st);
-        return launch_g2p_tiled<3, false, true>(A, n, st);
-    }
-    if (order == 1) return launch_g2p_tiled<1, false, false>(A, n, st);
-    if (order == 2) return launch_g2p_tiled<2, false, false>(A, n, st);
-    return launch_g2p_tiled<3, false, false>(A, n, st);
+    if (order == 1) return launch_g2p_order<1>(A, n, st, adv != nullptr, stag >= 0);
+    if (order == 2) return launch_g2p_order<2>(A, n, st, adv != nullptr, stag >= 0);
+    return launch_g2p_order<3>(A, n, st, adv != nullptr, stag >= 0);
 }
 
 }  // namespace pb
@@ -447,7 +471,7 @@ extern "C" picasso_status picasso_apic_p2g_update(
     gm.overflow = gmu.overflow = exec->overflow_count;
     bool handled = false;
     st = apic_p2g_tiled(mp, sd->order, 3, Form::F32Fixed, num_particles, x, m, c, gm, gmu, *bins,
-                        exec->error_count, s, &handled, &F);
+                        exec->error_count, s, &handled, &F, -1);
     if (st || handled) return st;
     // the tiled kernel does not take these particles (layout, tile size):
     // the fill of u above is overwritten by the separate update

@@ -34,6 +34,13 @@ namespace pb {
 constexpr int kStageLanes = 8;  // lanes staged per merge round
 constexpr unsigned kFull = 0xFFFFFFFFu;
 
+// Element type of the P2G node tile that sums the lanes' FP32 partials.
+#ifndef PB_P2G_TILE_F64
+#define PB_P2G_TILE_F64 0
+#endif
+using TileVal = std::conditional<PB_P2G_TILE_F64 != 0, double, float>::type;
+constexpr int kTileWords = sizeof(TileVal) / sizeof(float);
+
 struct TileP {
     int T[3];    // bins per tile
     int nt[3];   // tiles per dimension
@@ -55,6 +62,7 @@ struct TileP {
 struct P2GArgs {
     MeshP mp;
     TileP tp;
+    int stag;          // staggered location: the entity's dimension (else -1)
     const double* x;
     const float* rec;  // spline records (4 floats per particle) or null
     const float* m;
@@ -69,6 +77,7 @@ struct P2GArgs {
 struct G2PArgs {
     MeshP mp;
     TileP tp;
+    int stag;           // staggered location: the entity's dimension (else -1)
     const double* x;
     const float4* rec;  // spline records or null
     GField u;
@@ -188,9 +197,13 @@ __device__ __forceinline__ void cp_async_wait()
 // REC: the particle's position arrives as a spline record (in-cell fraction
 // of the logical position along each dimension in FP32, and the sort key
 // of its bin) instead of the FP64 position.
-template <int ORDER, int LPP, bool REC = false>
+// STAG: a staggered location (Face<D> / Edge<D>, APIC.hpp:148-232): two
+// grid fields, the mass and the one momentum component of the entity's
+// dimension, which comes from column `stag` of c_p.
+template <int ORDER, int LPP, bool REC = false, bool STAG = false>
 struct P2GCfg {
     static constexpr int K = SplineTraits<ORDER>::K;
+    static constexpr int NF = STAG ? 2 : 4;  // grid fields
     static constexpr int KKK = K * K * K;
     static constexpr int N0 = 1;  // centre knot of the quadratic and cubic stencils
     // Cubic stencils with 4 lanes per particle split the stencil by its
@@ -202,7 +215,7 @@ struct P2GCfg {
     static constexpr int NL = ISPLIT ? K * K : KKK;  // nodes per lane
     static constexpr int ROWS = NL / K;              // k-rows per lane
     static constexpr int FS = (NL + 3) & ~3;         // staged floats per field
-    static constexpr int F = ISPLIT ? 4 : 4 / LPP;   // fields per lane
+    static constexpr int F = ISPLIT ? NF : NF / LPP;  // fields per lane
     static constexpr int RUNS = 32 / LPP;            // runs per warp
     static constexpr int SV = F * FS;                // staged values per lane
     // staging stride: a multiple of 4 floats whose quarter is odd keeps the
@@ -232,6 +245,7 @@ struct P2GCfg {
     static constexpr int STAGE_OFF = DEPTH * RING;
     static constexpr int TILE_OFF = STAGE_OFF + kStageLanes * SS;
     static_assert(LPP == 1 || LPP == 2 || LPP == 4, "1, 2 or 4 lanes per particle");
+    static_assert(F >= 1, "at least one field per lane");
 };
 
 // Single-warp CTAs per SM the P2G register budget is sized for: 1 lane per
@@ -242,10 +256,11 @@ struct P2GOccupancy {
     static constexpr int value = LPP == 1 ? 8 : (LPP == 2 ? 12 : (ORDER == 3 ? 12 : 16));
 };
 
-template <int ORDER, int LPP, bool REC = false>
+template <int ORDER, int LPP, bool REC = false, bool STAG = false>
 __host__ __device__ constexpr int p2g_warp_floats(int P)
 {
-    return P2GCfg<ORDER, LPP, REC>::TILE_OFF + 4 * P;
+    return P2GCfg<ORDER, LPP, REC, STAG>::TILE_OFF +
+           P2GCfg<ORDER, LPP, REC, STAG>::NF * P * kTileWords;
 }
 
 // p + s g for a small integer s (s = 0: p exactly).  Called with unrolled
@@ -258,9 +273,9 @@ __device__ __forceinline__ float add_steps(int s, float p, float g)
     return fmaf((float)s, g, p);
 }
 
-template <int ORDER, int LPP>
+template <int ORDER, int LPP, bool STAG = false>
 struct P2GAcc {
-    using C = P2GCfg<ORDER, LPP>;
+    using C = P2GCfg<ORDER, LPP, false, STAG>;
     float acc[C::F][C::NL];
 
     __device__ __forceinline__ void zero()
@@ -290,22 +305,22 @@ struct P2GAcc {
                 if (i == h) wx = sp[0].w[i];
             const float wxm = wx * mass;
             const float hs = (float)(h - N0);
-            float pi[4];
+            float pi[C::F];
 #pragma unroll
-            for (int f = 1; f < 4; ++f) pi[f] = fmaf(hs, G[f][0], E[f]);
+            for (int f = 1; f < C::F; ++f) pi[f] = fmaf(hs, G[f][0], E[f]);
 #pragma unroll
             for (int j = 0; j < K; ++j) {
                 const float wij = wxm * sp[1].w[j];
-                float pij[4];
+                float pij[C::F];
 #pragma unroll
-                for (int f = 1; f < 4; ++f) pij[f] = add_steps(j - N0, pi[f], G[f][1]);
+                for (int f = 1; f < C::F; ++f) pij[f] = add_steps(j - N0, pi[f], G[f][1]);
 #pragma unroll
                 for (int k = 0; k < K; ++k) {
                     const int n = j * K + k;
                     const float w = wij * sp[2].w[k];
                     acc[0][n] += w;
 #pragma unroll
-                    for (int f = 1; f < 4; ++f)
+                    for (int f = 1; f < C::F; ++f)
                         acc[f][n] = fmaf(w, add_steps(k - N0, pij[f], G[f][2]), acc[f][n]);
                 }
             }
@@ -422,9 +437,9 @@ struct P2GAcc {
 // Merge plan of one lane: staged value v = lane + 32 r of a staged lane that
 // handles fields hh F .. hh F + F - 1 (plane split: i-plane hh) lands at tile
 // offset moff[r] + hh * fstride from the stencil start.
-template <int ORDER, int LPP>
+template <int ORDER, int LPP, bool STAG = false>
 struct MergePlan {
-    using C = P2GCfg<ORDER, LPP>;
+    using C = P2GCfg<ORDER, LPP, false, STAG>;
     int moff[C::R];
     int poff[C::RP];  // the same for the values of a k-plane stage
     int fstride;      // F * P (plane split: SI)
@@ -463,13 +478,14 @@ struct MergePlan {
 
 // Lanes in `mask` hand their partial sums to the warp's node tile in lane
 // order; their accumulators are zeroed.
-template <int ORDER, int LPP>
-__device__ __forceinline__ void merge_partials(unsigned mask, P2GAcc<ORDER, LPP>& acc,
-                                               int cur_base, const MergePlan<ORDER, LPP>& plan,
-                                               float* tile, float* stage, int* stage_base,
+template <int ORDER, int LPP, bool STAG>
+__device__ __forceinline__ void merge_partials(unsigned mask, P2GAcc<ORDER, LPP, STAG>& acc,
+                                               int cur_base,
+                                               const MergePlan<ORDER, LPP, STAG>& plan,
+                                               TileVal* tile, float* stage, int* stage_base,
                                                int lane)
 {
-    using C = P2GCfg<ORDER, LPP>;
+    using C = P2GCfg<ORDER, LPP, false, STAG>;
     while (mask) {
         unsigned batch = mask;
         if (__popc(mask) > kStageLanes) {  // the lowest kStageLanes lanes
@@ -504,12 +520,12 @@ __device__ __forceinline__ void merge_partials(unsigned mask, P2GAcc<ORDER, LPP>
 
 // Lanes in `mask` (whose bin moved one step along k) hand the first k-plane
 // of their sums to the node tile in lane order and shift the rest down.
-template <int ORDER, int LPP>
-__device__ __forceinline__ void merge_plane(unsigned mask, P2GAcc<ORDER, LPP>& acc, int cur_base,
-                                            const MergePlan<ORDER, LPP>& plan, float* tile,
-                                            float* stage, int* stage_base, int lane)
+template <int ORDER, int LPP, bool STAG>
+__device__ __forceinline__ void merge_plane(unsigned mask, P2GAcc<ORDER, LPP, STAG>& acc,
+                                            int cur_base, const MergePlan<ORDER, LPP, STAG>& plan,
+                                            TileVal* tile, float* stage, int* stage_base, int lane)
 {
-    using C = P2GCfg<ORDER, LPP>;
+    using C = P2GCfg<ORDER, LPP, false, STAG>;
     while (mask) {
         unsigned batch = mask;
         if (__popc(mask) > kStageLanes) {
@@ -582,13 +598,14 @@ __device__ __forceinline__ bool locate_record(const MeshP& mp, const TileP& tp, 
 // One P2G work item (tile t, particles [a, b)) by the calling warp.  `warp_smem`
 // holds p2g_warp_floats<ORDER, LPP, REC>(P) floats (16-byte aligned),
 // `stage_base` kStageLanes ints of shared memory.
-template <int ORDER, int LPP, bool REC = false>
+template <int ORDER, int LPP, bool REC = false, bool STAG = false>
 __device__ void p2g_item(const P2GArgs& A, int64_t t, int64_t a, int64_t b, float* warp_smem,
                          int* stage_base)
 {
-    using C = P2GCfg<ORDER, LPP, REC>;
-    using Acc = P2GAcc<ORDER, LPP>;
-    static_assert(C::SV == P2GCfg<ORDER, LPP>::SV && C::SS == P2GCfg<ORDER, LPP>::SS,
+    using C = P2GCfg<ORDER, LPP, REC, STAG>;
+    using Acc = P2GAcc<ORDER, LPP, STAG>;
+    static_assert(C::SV == P2GCfg<ORDER, LPP, false, STAG>::SV &&
+                      C::SS == P2GCfg<ORDER, LPP, false, STAG>::SS,
                   "the record form changes only the ring");
     constexpr int K = C::K;
     const MeshP& mp = A.mp;
@@ -597,7 +614,7 @@ __device__ void p2g_item(const P2GArgs& A, int64_t t, int64_t a, int64_t b, floa
     const int run = lane / LPP, h = lane % LPP;
     float* ring = warp_smem;
     float* stage = warp_smem + C::STAGE_OFF;
-    float* tile = warp_smem + C::TILE_OFF;
+    TileVal* tile = reinterpret_cast<TileVal*>(warp_smem + C::TILE_OFF);
 
     int ob[3];
     tile_origin(tp, t, ob);
@@ -627,8 +644,8 @@ __device__ void p2g_item(const P2GArgs& A, int64_t t, int64_t a, int64_t b, floa
         }
     }
 
-    for (int i = lane; i < 4 * tp.P; i += 32) tile[i] = 0.f;
-    MergePlan<ORDER, LPP> plan;
+    for (int i = lane; i < C::NF * tp.P; i += 32) tile[i] = TileVal(0);
+    MergePlan<ORDER, LPP, STAG> plan;
     plan.init(tp, lane);
     const float D = (ORDER >= 2) ? inertial_scaling<ORDER, float>(mp.dx[0]) : 1.f;
     const float Dh = D * (float)mp.dx[0];
@@ -700,7 +717,7 @@ __device__ void p2g_item(const P2GArgs& A, int64_t t, int64_t a, int64_t b, floa
         mass = sl[C::RING_M + run];
     };
     // cp[r * 3 + d] = c_p(r, d); field g of the lane: mass (g = 0) or
-    // momentum d = g - 1
+    // momentum d = g - 1 (staggered: d = the entity's dimension)
     auto centre_form = [&](const float cp[12], const Spline1D<ORDER, float> sp[3],
                            float E[C::F], float G[C::F][3]) {
 #pragma unroll
@@ -710,7 +727,7 @@ __device__ void p2g_item(const P2GArgs& A, int64_t t, int64_t a, int64_t b, floa
                 E[f] = 1.f;
                 G[f][0] = G[f][1] = G[f][2] = 0.f;
             } else {
-                const int d = g - 1;
+                const int d = STAG ? A.stag : g - 1;
                 const float bx = d == 0 ? cp[3] : (d == 1 ? cp[4] : cp[5]);
                 const float by = d == 0 ? cp[6] : (d == 1 ? cp[7] : cp[8]);
                 const float bz = d == 0 ? cp[9] : (d == 1 ? cp[10] : cp[11]);
@@ -732,7 +749,7 @@ __device__ void p2g_item(const P2GArgs& A, int64_t t, int64_t a, int64_t b, floa
                 co[f][0] = 1.f;
                 co[f][1] = co[f][2] = co[f][3] = 0.f;
             } else {
-                const int d = g - 1;
+                const int d = STAG ? A.stag : g - 1;
                 co[f][0] = d == 0 ? cp[0] : (d == 1 ? cp[1] : cp[2]);
                 co[f][1] = d == 0 ? cp[3] : (d == 1 ? cp[4] : cp[5]);
                 co[f][2] = d == 0 ? cp[6] : (d == 1 ? cp[7] : cp[8]);
@@ -760,8 +777,8 @@ __device__ void p2g_item(const P2GArgs& A, int64_t t, int64_t a, int64_t b, floa
         const bool kstep = chg && lbin == cur + 1 && lb[2] != 0;
         const unsigned pm = __ballot_sync(kFull, kstep);
         const unsigned fm = __ballot_sync(kFull, chg && !kstep);
-        if (pm) merge_plane<ORDER, LPP>(pm, acc, cur_base, plan, tile, stage, stage_base, lane);
-        if (fm) merge_partials<ORDER, LPP>(fm, acc, cur_base, plan, tile, stage, stage_base, lane);
+        if (pm) merge_plane(pm, acc, cur_base, plan, tile, stage, stage_base, lane);
+        if (fm) merge_partials(fm, acc, cur_base, plan, tile, stage, stage_base, lane);
         if (ok) {
             if (lbin != cur) {
                 cur = lbin;
@@ -782,7 +799,7 @@ __device__ void p2g_item(const P2GArgs& A, int64_t t, int64_t a, int64_t b, floa
     }
     cp_async_wait<0>();
     const unsigned fm = __ballot_sync(kFull, cur >= 0);
-    if (fm) merge_partials<ORDER, LPP>(fm, acc, cur_base, plan, tile, stage, stage_base, lane);
+    if (fm) merge_partials(fm, acc, cur_base, plan, tile, stage, stage_base, lane);
     // the item's node box, rounded to fixed point and added to HBM (nodes
     // that received nothing are skipped)
     if (__any_sync(kFull, cur >= 0)) {
@@ -797,14 +814,14 @@ __device__ void p2g_item(const P2GArgs& A, int64_t t, int64_t a, int64_t b, floa
             const int gj = node_global(mp, tp, 1, ob[1], j);
             const int gk = node_global(mp, tp, 2, ob[2], k);
 #pragma unroll
-            for (int f = 0; f < 4; ++f) {
-                const float v = tile[f * tp.P + idx];
-                if (v != 0.f) {
-                    const long long q =
-                        to_fixed(f == 0 ? A.gm : A.gmu, v * (f == 0 ? A.scale_m : A.scale_mu));
+            for (int f = 0; f < C::NF; ++f) {
+                const TileVal v = tile[f * tp.P + idx];
+                if (v != TileVal(0)) {
+                    const long long q = to_fixed(
+                        f == 0 ? A.gm : A.gmu, v * (TileVal)(f == 0 ? A.scale_m : A.scale_mu));
                     unsigned long long* dst = reinterpret_cast<unsigned long long*>(
                         f == 0 ? A.gm.ptr<long long>(gi, gj, gk, 0)
-                               : A.gmu.ptr<long long>(gi, gj, gk, f - 1));
+                               : A.gmu.ptr<long long>(gi, gj, gk, STAG ? 0 : f - 1));
                     atomicAdd(dst, (unsigned long long)q);
                 }
             }
@@ -983,11 +1000,16 @@ __global__ void zero_untouched_regions_kernel(MeshP mp, TileP tp, FusedUpdate F)
 // The positions of the item's first and last particle are read before the
 // tile barrier, so no thread reads a position another thread has moved.
 // REC: the particles' splines come from their records (not with ADV).
-template <int ORDER, int NTHR, bool ADV = false, bool REC = false>
+// STAG: a staggered location (APIC.hpp:477-544): the grid field is the scalar
+// velocity component of the entity's dimension, which lands in column `stag`
+// of c_p (the other columns are written as zero, as the plain kernel does).
+template <int ORDER, int NTHR, bool ADV = false, bool REC = false, bool STAG = false>
 __device__ void g2p_item(const G2PArgs& A, int64_t t, int64_t a, int64_t b, float4* tile,
                          int tid)
 {
     static_assert(!(ADV && REC), "the advection reads the FP64 positions");
+    static_assert(!(ADV && STAG), "the advection moves by the 3-component velocity");
+    constexpr int NU = STAG ? 1 : 3;  // velocity components gathered
     constexpr int K = SplineTraits<ORDER>::K;
     constexpr int N0 = ORDER == 1 ? 0 : 1;  // centre knot of the stencil
     const MeshP& mp = A.mp;
@@ -1038,8 +1060,10 @@ __device__ void g2p_item(const G2PArgs& A, int64_t t, int64_t a, int64_t b, floa
         float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
         if (inside) {  // through L2: the batched kernel writes u_i in the same launch
             v.x = __ldcg(A.u.ptr<float>(gi, gj, gk, 0));
-            v.y = __ldcg(A.u.ptr<float>(gi, gj, gk, 1));
-            v.z = __ldcg(A.u.ptr<float>(gi, gj, gk, 2));
+            if (!STAG) {
+                v.y = __ldcg(A.u.ptr<float>(gi, gj, gk, 1));
+                v.z = __ldcg(A.u.ptr<float>(gi, gj, gk, 2));
+            }
         }
         tile[(i * tp.NT[1] + j) * tp.NT[2] + k] = v;
     }
@@ -1100,7 +1124,7 @@ __device__ void g2p_item(const G2PArgs& A, int64_t t, int64_t a, int64_t b, floa
                     const float4 ue = row[k];
                     const float uk[3] = {ue.x, ue.y, ue.z};
 #pragma unroll
-                    for (int d = 0; d < 3; ++d) {
+                    for (int d = 0; d < NU; ++d) {
                         const float wu = sp[2].w[k] * uk[d];
                         S0[d] += wu;
                         S1[d] = add_steps(k - N0, S1[d], wu);
@@ -1108,7 +1132,7 @@ __device__ void g2p_item(const G2PArgs& A, int64_t t, int64_t a, int64_t b, floa
                 }
                 const float wy = sp[1].w[j];
 #pragma unroll
-                for (int d = 0; d < 3; ++d) {
+                for (int d = 0; d < NU; ++d) {
                     const float wS0 = wy * S0[d];
                     A0[d] += wS0;
                     A1[d] = add_steps(j - N0, A1[d], wS0);
@@ -1117,7 +1141,7 @@ __device__ void g2p_item(const G2PArgs& A, int64_t t, int64_t a, int64_t b, floa
             }
             const float wx = sp[0].w[i];
 #pragma unroll
-            for (int d = 0; d < 3; ++d) {
+            for (int d = 0; d < NU; ++d) {
                 const float wA0 = wx * A0[d];
                 up[d] += wA0;
                 M[d][0] = add_steps(i - N0, M[d][0], wA0);
@@ -1127,10 +1151,21 @@ __device__ void g2p_item(const G2PArgs& A, int64_t t, int64_t a, int64_t b, floa
         }
         float B[3][3];
 #pragma unroll
-        for (int d = 0; d < 3; ++d)
+        for (int d = 0; d < NU; ++d)
 #pragma unroll
             for (int q = 0; q < 3; ++q)
                 B[d][q] = fmaf((float)mp.dx[q], M[d][q], sp[q].d[N0] * up[d]);
+        if constexpr (STAG) {
+            // the gathered component belongs to column stag; the others are 0
+            const float u0 = up[0], b0[3] = {B[0][0], B[0][1], B[0][2]};
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const bool mine = d == A.stag;
+                up[d] = mine ? u0 : 0.f;
+#pragma unroll
+                for (int q = 0; q < 3; ++q) B[d][q] = mine ? b0[q] : 0.f;
+            }
+        }
         // c_p(0, d) = u_p(d); c_p(1 + q, d) = B_p(d, q)  (APIC.hpp:464-471)
         float4* out = reinterpret_cast<float4*>(A.c + 12 * p);
         out[0] = make_float4(up[0], up[1], up[2], B[0][0]);
@@ -1145,13 +1180,14 @@ __device__ void g2p_item(const G2PArgs& A, int64_t t, int64_t a, int64_t b, floa
 
 // host helpers (tiled.cu)
 bool fused_update_fits(const TileP& tp, int order);
-bool make_tilep(const MeshP& mp, int order, const picasso_bins& bins, TileP* tp, int lpp = 0);
+bool make_tilep(const MeshP& mp, int order, const picasso_bins& bins, TileP* tp, int lpp = 0,
+                int nf = 4);
 int device_smem_optin();
 bool packed_x(const PField& x);
 bool packed_m(const PField& m);
 bool packed_c(const PField& c);
 int default_lpp(int order);
-bool valid_lpp(int order, int lpp);
-size_t p2g_warp_bytes(int order, int lpp, int P, bool rec = false);
+bool valid_lpp(int order, int lpp, bool stag = false);
+size_t p2g_warp_bytes(int order, int lpp, int P, bool rec = false, bool stag = false);
 
 }  // namespace pb

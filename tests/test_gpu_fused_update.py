@@ -120,4 +120,6 @@ def test_untouched_nodes_get_zero_velocity(cuda):
     c = np.concatenate([rng.standard_normal((4000, 1, 3)),
                         0.1 * rng.standard_normal((4000, 3, 3))], axis=1)
     u = _compare(mesh, 2, x, m, c, (4, 4, 4), records=False, dt=1e-3)
-    assert float(u[16:, 16:, 16:].abs().max()) == 0.0
+    # the stencils reach nodes 23 (wrapped) .. 7 along each dimension
+    assert float(u[9:22, 9:22, 9:22].abs().max()) == 0.0
+    assert float(u[:7, :7, :7].abs().max()) > 0.0

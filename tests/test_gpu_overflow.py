@@ -20,9 +20,10 @@ from picasso_b200 import (APIC, FieldLocation, FixedGrid, cell_sort, create_spli
 pytestmark = pytest.mark.gpu
 
 
-def _p2g(bits, mass_scale, ppc, tiled):
+def _p2g(bits, mass_scale, ppc, tiled, c_scale=1.0):
     mesh = periodic_mesh(12, halo=0)
     x, m, c = uniform_particles(mesh, ppc, seed=91, jitter_mass=False)
+    c = c * c_scale
     xd = torch.as_tensor(x, device="cuda")
     md = torch.as_tensor(m * mass_scale, dtype=torch.float32, device="cuda")
     cd = torch.as_tensor(c, dtype=torch.float32, device="cuda").contiguous()
@@ -61,10 +62,11 @@ def test_contributions_beyond_range_are_counted(cuda, tiled):
 
 @pytest.mark.parametrize("update", [False, True])
 def test_wrapped_mass_sums_are_counted(cuda, update):
-    # unit masses, 61 bits: every contribution is in range (w <= 0.42), but a
-    # node's mass (about 6 at 6 particles per cell) is above 2^(63-61) = 4, so
-    # its 64-bit sum wraps negative
-    mesh, gm, gmu, n = _p2g(61, 1.0, 6, tiled=False)
+    # unit masses and small velocities, 61 bits: every contribution is in
+    # range (|value| < 2: w <= 0.42, momenta scaled down), but a node's mass
+    # (about 6 at 6 particles per cell) is above 2^(63-61) = 4, so its 64-bit
+    # sum wraps negative
+    mesh, gm, gmu, n = _p2g(61, 1.0, 6, tiled=False, c_scale=0.01)
     assert n == 0
     assert int((gm.raw < 0).sum().item()) > 0
     desc = mesh.descriptor(FieldLocation.Node)
