@@ -23,6 +23,14 @@
 // G2P item (one warp or one CTA): the item's node velocities are staged once
 // in a shared float4 tile and every thread gathers its particles' stencils
 // from there, contracting the stencil one dimension at a time.
+//
+// Both read either the FP64 positions or, when the bins carry them, spline
+// records (in-cell fractions as FP32 + sort key, written by
+// picasso_spline_records from the same FP64 arithmetic): same splines and
+// bins, 16 instead of 24 bytes per particle, no FP64 instruction.  Staggered
+// locations (Face / Edge) accumulate two grid fields (mass and the entity's
+// momentum component) instead of four.  The P2G can also apply the grid
+// update to the nodes whose sums are complete (fused_update_arrive).
 #pragma once
 
 #include "common.cuh"
