@@ -201,14 +201,17 @@ def _errs(got, ref, mask=None):
     sel = dd > 0
     if mask is not None:
         sel &= mask
-    pe = float((num[sel] / dd[sel]).max()) if sel.any() else 0.0
-    return {"normwise": nw, "per_entry": pe}
+    rel = num[sel] / dd[sel]
+    pe = float(rel.max()) if sel.any() else 0.0
+    return {"normwise": nw, "per_entry": pe, "entries": int(sel.sum()),
+            "entries_above_1e-5": int(np.count_nonzero(rel > 1e-5))}
 
 
 def gpu_errors_vs_oracle(args, mesh, x, m, c, grids, c_ref):
     """Errors of the GPU forms against the oracle's FP64 step on the CPU
-    sample: FP32 form (tiled kernels on cell-sorted particles, the headline
-    path) and FP64 plain form (unsorted particles)."""
+    sample: FP32 form (tiled kernels on cell-sorted particles with spline
+    records, the headline path; and the plain fixed-point kernel) and FP64
+    plain form (unsorted particles)."""
     import torch
 
     import picasso_b200 as pb
@@ -230,6 +233,8 @@ def gpu_errors_vs_oracle(args, mesh, x, m, c, grids, c_ref):
                                     torch.as_tensor(c, dtype=torch.float32,
                                                     device="cuda").contiguous())
     sds = pb.create_spline(loc, args.order, mesh, xs)
+    if not args.no_records:
+        pb.spline_records(sds, bins)
     acc = torch.zeros(ext + (4,), dtype=torch.int64, device="cuda")
     gm, gmu = pb.FixedGrid(acc[..., 0], FIXED_BITS), pb.FixedGrid(acc[..., 1:], FIXED_BITS)
     u = torch.zeros(ext + (3,), dtype=torch.float32, device="cuda")
@@ -244,6 +249,21 @@ def gpu_errors_vs_oracle(args, mesh, x, m, c, grids, c_ref):
                          "grid_velocity": _errs(u.double().cpu().numpy(), gu_o, heavy),
                          "particle_velocity": _errs(cb[:, 0], c_ref[:, 0]),
                          "particle_affine": _errs(cb[:, 1:], c_ref[:, 1:])}
+    # FP32 form, plain fixed-point kernel on the unsorted particles
+    sd = pb.create_spline(loc, args.order, mesh, xd)
+    accp = torch.zeros(ext + (4,), dtype=torch.int64, device="cuda")
+    gmp, gmup = pb.FixedGrid(accp[..., 0], FIXED_BITS), pb.FixedGrid(accp[..., 1:], FIXED_BITS)
+    up = torch.zeros(ext + (3,), dtype=torch.float32, device="cuda")
+    cp_ = torch.as_tensor(c, dtype=torch.float32, device="cuda").contiguous()
+    pb.APIC.p2g(torch.as_tensor(m, dtype=torch.float32, device="cuda"), cp_, gmp, gmup, sd)
+    pb.grid_velocity(sd.desc.mesh, gmp, gmup, up, 1e-12)
+    pb.APIC.g2p(up, cp_, sd)
+    cph = cp_.double().cpu().numpy()
+    res["fp32_plain"] = {"grid_mass": _errs(gmp.to_float().cpu().numpy(), gm_o, heavy),
+                         "grid_momentum": _errs(gmup.to_float().cpu().numpy(), gmu_o, heavy),
+                         "grid_velocity": _errs(up.double().cpu().numpy(), gu_o, heavy),
+                         "particle_velocity": _errs(cph[:, 0], c_ref[:, 0]),
+                         "particle_affine": _errs(cph[:, 1:], c_ref[:, 1:])}
     # FP64 plain form, unsorted
     sd = pb.create_spline(loc, args.order, mesh, xd)
     g64 = torch.zeros(ext + (4,), dtype=torch.float64, device="cuda")

