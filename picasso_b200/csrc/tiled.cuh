@@ -484,6 +484,71 @@ struct MergePlan {
     }
 };
 
+// The warp adds the values of `nstage` staged lanes (slot q: stage + q SLOT,
+// its base in stage_base[q]) into the node tile: lane l adds value l + 32 r
+// of each slot at tile offset base + off[r], slot after slot (a fixed order,
+// so the tile sums are reproducible).
+#ifndef PB_P2G_MERGE
+#define PB_P2G_MERGE 0
+#endif
+template <int NR, int SLOT, int LPP>
+__device__ __forceinline__ void add_staged(int nstage, const float* stage, const int* stage_base,
+                                           const int (&off)[NR], unsigned valid, int fstride,
+                                           TileVal* tile, int lane)
+{
+#if PB_P2G_MERGE == 1
+    // bases of every slot and the next slot's values are loaded ahead, so
+    // each slot costs one tile load -> add -> store
+    int sb[kStageLanes];
+#pragma unroll
+    for (int q = 0; q < kStageLanes; ++q) sb[q] = stage_base[q];
+    float v[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) v[r] = ((valid >> r) & 1u) ? stage[lane + 32 * r] : 0.f;
+#pragma unroll
+    for (int q = 0; q < kStageLanes; ++q) {
+        if (q < nstage) {
+            float nv[NR];
+#pragma unroll
+            for (int r = 0; r < NR; ++r)
+                nv[r] = (q + 1 < nstage && ((valid >> r) & 1u))
+                            ? stage[(q + 1) * SLOT + lane + 32 * r] : 0.f;
+            const int base = (sb[q] & 0x0FFFFFFF) + (LPP > 1 ? (sb[q] >> 28) * fstride : 0);
+#pragma unroll
+            for (int r = 0; r < NR; ++r)
+                if ((valid >> r) & 1u) tile[base + off[r]] += v[r];
+            __syncwarp();
+#pragma unroll
+            for (int r = 0; r < NR; ++r) v[r] = nv[r];
+        }
+    }
+#elif PB_P2G_MERGE == 2
+    // shared-memory reductions, issued slot after slot
+#pragma unroll
+    for (int q = 0; q < kStageLanes; ++q) {
+        if (q < nstage) {
+            const int sb = stage_base[q];
+            const int base = (sb & 0x0FFFFFFF) + (LPP > 1 ? (sb >> 28) * fstride : 0);
+#pragma unroll
+            for (int r = 0; r < NR; ++r)
+                if ((valid >> r) & 1u)
+                    atomicAdd(tile + base + off[r], (TileVal)stage[q * SLOT + lane + 32 * r]);
+        }
+    }
+    __syncwarp();
+#else
+    for (int q = 0; q < nstage; ++q) {
+        const float* st = stage + q * SLOT;
+        const int sb = stage_base[q];
+        const int base = (sb & 0x0FFFFFFF) + (LPP > 1 ? (sb >> 28) * fstride : 0);
+#pragma unroll
+        for (int r = 0; r < NR; ++r)
+            if ((valid >> r) & 1u) tile[base + off[r]] += st[lane + 32 * r];
+        __syncwarp();
+    }
+#endif
+}
+
 // Lanes in `mask` hand their partial sums to the warp's node tile in lane
 // order; their accumulators are zeroed.
 template <int ORDER, int LPP, bool STAG>
@@ -513,16 +578,8 @@ __device__ __forceinline__ void merge_partials(unsigned mask, P2GAcc<ORDER, LPP,
             acc.zero();
         }
         __syncwarp();
-        const int nstage = __popc(batch);
-        for (int q = 0; q < nstage; ++q) {
-            const float* st = stage + q * C::SS;
-            const int sb = stage_base[q];
-            const int base = (sb & 0x0FFFFFFF) + (LPP > 1 ? (sb >> 28) * plan.fstride : 0);
-#pragma unroll
-            for (int r = 0; r < C::R; ++r)
-                if ((plan.valid >> r) & 1u) tile[base + plan.moff[r]] += st[lane + 32 * r];
-            __syncwarp();
-        }
+        add_staged<C::R, C::SS, LPP>(__popc(batch), stage, stage_base, plan.moff, plan.valid,
+                                     plan.fstride, tile, lane);
     }
 }
 
@@ -553,16 +610,8 @@ __device__ __forceinline__ void merge_plane(unsigned mask, P2GAcc<ORDER, LPP, ST
             acc.shift_k();
         }
         __syncwarp();
-        const int nstage = __popc(batch);
-        for (int q = 0; q < nstage; ++q) {
-            const float* st = stage + q * C::PS;
-            const int sb = stage_base[q];
-            const int base = (sb & 0x0FFFFFFF) + (LPP > 1 ? (sb >> 28) * plan.fstride : 0);
-#pragma unroll
-            for (int r = 0; r < C::RP; ++r)
-                if ((plan.pvalid >> r) & 1u) tile[base + plan.poff[r]] += st[lane + 32 * r];
-            __syncwarp();
-        }
+        add_staged<C::RP, C::PS, LPP>(__popc(batch), stage, stage_base, plan.poff, plan.pvalid,
+                                      plan.fstride, tile, lane);
     }
 }
 
