@@ -488,55 +488,11 @@ struct MergePlan {
 // its base in stage_base[q]) into the node tile: lane l adds value l + 32 r
 // of each slot at tile offset base + off[r], slot after slot (a fixed order,
 // so the tile sums are reproducible).
-#ifndef PB_P2G_MERGE
-#define PB_P2G_MERGE 0
-#endif
 template <int NR, int SLOT, int LPP>
 __device__ __forceinline__ void add_staged(int nstage, const float* stage, const int* stage_base,
                                            const int (&off)[NR], unsigned valid, int fstride,
                                            TileVal* tile, int lane)
 {
-#if PB_P2G_MERGE == 1
-    // bases of every slot and the next slot's values are loaded ahead, so
-    // each slot costs one tile load -> add -> store
-    int sb[kStageLanes];
-#pragma unroll
-    for (int q = 0; q < kStageLanes; ++q) sb[q] = stage_base[q];
-    float v[NR];
-#pragma unroll
-    for (int r = 0; r < NR; ++r) v[r] = ((valid >> r) & 1u) ? stage[lane + 32 * r] : 0.f;
-#pragma unroll
-    for (int q = 0; q < kStageLanes; ++q) {
-        if (q < nstage) {
-            float nv[NR];
-#pragma unroll
-            for (int r = 0; r < NR; ++r)
-                nv[r] = (q + 1 < nstage && ((valid >> r) & 1u))
-                            ? stage[(q + 1) * SLOT + lane + 32 * r] : 0.f;
-            const int base = (sb[q] & 0x0FFFFFFF) + (LPP > 1 ? (sb[q] >> 28) * fstride : 0);
-#pragma unroll
-            for (int r = 0; r < NR; ++r)
-                if ((valid >> r) & 1u) tile[base + off[r]] += v[r];
-            __syncwarp();
-#pragma unroll
-            for (int r = 0; r < NR; ++r) v[r] = nv[r];
-        }
-    }
-#elif PB_P2G_MERGE == 2
-    // shared-memory reductions, issued slot after slot
-#pragma unroll
-    for (int q = 0; q < kStageLanes; ++q) {
-        if (q < nstage) {
-            const int sb = stage_base[q];
-            const int base = (sb & 0x0FFFFFFF) + (LPP > 1 ? (sb >> 28) * fstride : 0);
-#pragma unroll
-            for (int r = 0; r < NR; ++r)
-                if ((valid >> r) & 1u)
-                    atomicAdd(tile + base + off[r], (TileVal)stage[q * SLOT + lane + 32 * r]);
-        }
-    }
-    __syncwarp();
-#else
     for (int q = 0; q < nstage; ++q) {
         const float* st = stage + q * SLOT;
         const int sb = stage_base[q];
@@ -546,7 +502,6 @@ __device__ __forceinline__ void add_staged(int nstage, const float* stage, const
             if ((valid >> r) & 1u) tile[base + off[r]] += st[lane + 32 * r];
         __syncwarp();
     }
-#endif
 }
 
 // Lanes in `mask` hand their partial sums to the warp's node tile in lane
