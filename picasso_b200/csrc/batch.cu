@@ -504,6 +504,9 @@ picasso_status make_instance(const picasso_batch_instance& in, bool f32, BInst* 
     I->p2g.scale_mu = f32 ? ldexpf(1.f, in.mu_i.fixed_bits) : 0.f;
     I->p2g.err = in.error_count;
     I->p2g.stag = -1;
+    // element-wise flush: in the fused launch the next phase's items read the
+    // accumulators once the P2G items have counted themselves done
+    I->p2g.bulk_flush = 0;
     I->g2p.mp = mp;
     I->g2p.tp = tp;
     I->g2p.x = I->p2g.x;

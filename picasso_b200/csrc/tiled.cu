@@ -263,9 +263,13 @@ static int64_t item_bound(const TileP& tp, int64_t n)
 }
 
 template <int ORDER, int LPP, bool REC, bool STAG>
-static picasso_status launch_p2g_tiled(const P2GArgs& A, const FusedUpdate* fu, int64_t n,
+static picasso_status launch_p2g_tiled(const P2GArgs& args, const FusedUpdate* fu, int64_t n,
                                        cudaStream_t st)
 {
+    P2GArgs A = args;
+    // the bulk flush rounds rows into the ring and staging area: one k-row
+    // at least must fit
+    if (P2GCfg<ORDER, LPP, REC, STAG>::TILE_OFF / 8 < A.tp.NT[2]) A.bulk_flush = 0;
     const size_t smem = p2g_warp_bytes(ORDER, LPP, A.tp.P, REC, STAG);
     const int64_t items = item_bound(A.tp, n);
     if constexpr (!STAG) {
@@ -297,6 +301,16 @@ static picasso_status launch_g2p_tiled(const G2PArgs& A, int64_t n, cudaStream_t
     g2p_tiled_kernel<ORDER, ADV, REC, STAG>
         <<<(unsigned)(items ? items : 1), G2PThreads<ORDER>::value, smem, st>>>(A, n);
     return check_launch();
+}
+
+// gm and gmu are views of one (..., 4) 64-bit accumulator: a node's mass and
+// momentum are 4 consecutive words, nodes 16-byte aligned, a k-row of nodes
+// contiguous.
+static bool packed_accumulator(const GField& gm, const GField& gmu)
+{
+    return gmu.data == gm.data + sizeof(long long) && gm.s[2] == 4 && gmu.s[2] == 4 &&
+           gm.s[0] == gmu.s[0] && gm.s[1] == gmu.s[1] && gmu.s[3] == 1 && gm.s[0] % 2 == 0 &&
+           gm.s[1] % 2 == 0 && reinterpret_cast<uintptr_t>(gm.data) % 16 == 0;
 }
 
 // Spline records the tiled kernels may read instead of the positions: a
@@ -337,6 +351,8 @@ picasso_status apic_p2g_tiled(const MeshP& mp, int order, int ncomp, Form form, 
     A.scale_m = ldexpf(1.f, gm.fixed_bits);
     A.scale_mu = ldexpf(1.f, gmu.fixed_bits);
     A.err = err;
+    // the fused update counts its arrivals after element-wise reductions
+    A.bulk_flush = !sg && !fu && packed_accumulator(gm, gmu);
 #define PB_CASE(O, L, S)                                                                \
     if (order == O && lpp == L && sg == S)                                              \
         return rec ? launch_p2g_tiled<O, L, true, S>(A, fu, n, st)                      \

@@ -80,6 +80,10 @@ struct P2GArgs {
     float scale_m;
     float scale_mu;
     int* err;
+    // gm and gmu are one packed accumulator (a node's mass and momentum are 4
+    // consecutive 64-bit words, 16-byte aligned): the item's flush adds whole
+    // k-rows with bulk reductions (flush_rows_bulk)
+    int bulk_flush;
 };
 
 struct G2PArgs {
@@ -186,6 +190,29 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait()
 {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+// ---------------------------------------------------------------------------
+// bulk reductions (shared -> global through the tensor memory accelerator;
+// both addresses 16-byte aligned, size a multiple of 16 bytes)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void bulk_add_u64(long long* dst, const long long* src, int bytes)
+{
+    asm volatile("cp.reduce.async.bulk.global.shared::cta.bulk_group.add.u64 [%0], [%1], %2;\n"
+                 ::"l"(dst), "r"(smem_addr(src)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
+// the shared-memory sources of this thread's committed bulk operations have
+// been read (the buffer may be rewritten)
+__device__ __forceinline__ void bulk_wait_read()
+{
+    asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");
+}
+// shared-memory writes of this thread become visible to the bulk operations
+__device__ __forceinline__ void fence_proxy_async_smem()
+{
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
 }
 
 // ---------------------------------------------------------------------------
@@ -607,6 +634,75 @@ __device__ __forceinline__ bool locate_record(const MeshP& mp, const TileP& tp, 
     return ok;
 }
 
+// Flush of a P2G item's node box (bin rows [i_lo, i_hi] plus the halo, the
+// whole tile along j and k) into a packed accumulator: the box's k-rows are
+// rounded to fixed point into `buf` (room for buf_nodes nodes of 4 words, a
+// group of rows at a time) and each row is added to HBM by one bulk
+// reduction (two where it wraps around a periodic boundary; rows and nodes
+// past a non-periodic mesh end are left out -- no stencil reaches them).
+// The integer sums do not depend on the order of the reductions.
+template <int ORDER>
+__device__ __forceinline__ void flush_rows_bulk(const P2GArgs& A, const TileVal* tile, int i_lo,
+                                                int i_hi, const int ob[3], float* buf_f,
+                                                int buf_nodes, int lane)
+{
+    constexpr int K = SplineTraits<ORDER>::K;
+    const MeshP& mp = A.mp;
+    const TileP& tp = A.tp;
+    long long* buf = reinterpret_cast<long long*>(buf_f);
+    const int e1 = tp.NT[1], e2 = tp.NT[2];
+    const int rows = (i_hi - i_lo + K) * e1;
+    const int per = buf_nodes / e2;  // rows per group (>= 1, checked by the host)
+    // nodes of a row before the periodic wrap or the mesh end along k
+    const int gk0 = node_global(mp, tp, 2, ob[2], 0);
+    const int n0 = mp.periodic[2] ? min(e2, tp.nb[2] - ob[2]) : min(e2, mp.ext[2] - gk0);
+    const bool wraps = mp.periodic[2] && n0 < e2;
+    const int gk1 = wraps ? node_global(mp, tp, 2, ob[2], n0) : 0;
+    for (int r0 = 0; r0 < rows; r0 += per) {
+        const int nr = min(per, rows - r0);
+        if (r0 > 0) {  // the previous group's rows have been read
+            bulk_wait_read();
+            __syncwarp();
+        }
+        for (int node = lane; node < nr * e2; node += 32) {  // node of the group
+            const int q = node / e2;
+            const int k = node - q * e2;
+            const int row = r0 + q;
+            const int i = i_lo + row / e1, j = row - (row / e1) * e1;
+            const int idx = i * tp.SI + j * tp.SJ + k;
+            long long w[4];
+#pragma unroll
+            for (int f = 0; f < 4; ++f) {
+                const TileVal x = tile[f * tp.P + idx];
+                w[f] = x != TileVal(0)
+                           ? to_fixed(f == 0 ? A.gm : A.gmu,
+                                      x * (TileVal)(f == 0 ? A.scale_m : A.scale_mu))
+                           : 0LL;
+            }
+            longlong2* d = reinterpret_cast<longlong2*>(buf + 4 * node);
+            d[0] = make_longlong2(w[0], w[1]);
+            d[1] = make_longlong2(w[2], w[3]);
+        }
+        fence_proxy_async_smem();
+        __syncwarp();
+        for (int q = lane; q < nr; q += 32) {
+            const int row = r0 + q;
+            const int i = i_lo + row / e1, j = row - (row / e1) * e1;
+            const int gi = node_global(mp, tp, 0, ob[0], i);
+            const int gj = node_global(mp, tp, 1, ob[1], j);
+            if ((!mp.periodic[0] && gi >= mp.ext[0]) || (!mp.periodic[1] && gj >= mp.ext[1]))
+                continue;
+            const long long* src = buf + (size_t)q * e2 * 4;
+            if (n0 > 0) bulk_add_u64(A.gm.ptr<long long>(gi, gj, gk0, 0), src, n0 * 32);
+            if (wraps)
+                bulk_add_u64(A.gm.ptr<long long>(gi, gj, gk1, 0), src + 4 * n0, (e2 - n0) * 32);
+        }
+        bulk_commit();
+    }
+    bulk_wait_read();  // the buffer is the next item's ring
+    __syncwarp();
+}
+
 // One P2G work item (tile t, particles [a, b)) by the calling warp.  `warp_smem`
 // holds p2g_warp_floats<ORDER, LPP, REC>(P) floats (16-byte aligned),
 // `stage_base` kStageLanes ints of shared memory.
@@ -812,9 +908,13 @@ __device__ void p2g_item(const P2GArgs& A, int64_t t, int64_t a, int64_t b, floa
     cp_async_wait<0>();
     const unsigned fm = __ballot_sync(kFull, cur >= 0);
     if (fm) merge_partials(fm, acc, cur_base, plan, tile, stage, stage_base, lane);
-    // the item's node box, rounded to fixed point and added to HBM (nodes
-    // that received nothing are skipped)
-    if (__any_sync(kFull, cur >= 0)) {
+    // the item's node box, rounded to fixed point and added to HBM: by bulk
+    // reductions of whole k-rows into a packed accumulator (the ring and the
+    // staging area hold the rounded rows), else node by node (nodes that
+    // received nothing are skipped)
+    if (!STAG && A.bulk_flush && __any_sync(kFull, cur >= 0)) {
+        flush_rows_bulk<ORDER>(A, tile, i_lo, i_hi, ob, warp_smem, C::TILE_OFF / 8, lane);
+    } else if (__any_sync(kFull, cur >= 0)) {
         const int e1 = tp.NT[1], e2 = tp.NT[2];
         const int total = (i_hi - i_lo + K) * e1 * e2;
         for (int e = lane; e < total; e += 32) {
