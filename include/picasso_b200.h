@@ -356,6 +356,54 @@ PICASSO_API picasso_status picasso_apic_g2p_advect_keys(const picasso_spline* sd
                                                         const picasso_exec* exec);
 
 /* ------------------------------------------------------------------------ */
+/* Halo exchange inside the transfers (slab decomposition along x)          */
+/* ------------------------------------------------------------------------ */
+
+/* Neighbour grids of a rank whose local mesh is a slab of x-planes with
+ * ghost planes on either side.  Local x-planes p < lo_end belong to the lower
+ * neighbour (its plane p + lo_shift), planes p >= hi_begin to the upper one
+ * (its plane p + hi_shift).  The neighbour grids have this rank's strides and
+ * dtypes and must be addressable from this device (the same device, or a
+ * peer GPU's memory mapped here, e.g. by CUDA IPC with peer access).
+ * P2G: lo[0] / hi[0] are the neighbours' m_i, lo[1] / hi[1] their mu_i.
+ * G2P: lo[0] / hi[0] are the neighbours' u_i. */
+typedef struct picasso_halo_peers {
+    int32_t lo_end;
+    int32_t hi_begin;
+    int32_t lo_shift;
+    int32_t hi_shift;
+    void* lo[2];
+    void* hi[2];
+} picasso_halo_peers;
+
+/* picasso_apic_p2g whose contributions to ghost-plane nodes are added
+ * directly into the neighbour that owns them (64-bit integer reductions, over
+ * NVLink for a peer GPU): once every rank's call has completed, each rank's
+ * owned planes hold the complete sums and its ghost planes are untouched.
+ * This is the reference's P2G followed by the halo scatter with Sum
+ * (Picasso_FieldManager.hpp:157-164) in one pass.  Tiled FP32 form only
+ * (exec->bins, F32 particle fields, I64_FIXED grids, collocated Node
+ * location, packed particle storage); anything else returns
+ * PICASSO_ERR_UNSUPPORTED. */
+PICASSO_API picasso_status picasso_apic_p2g_halo(const picasso_spline* sd, int64_t num_particles,
+                                                 picasso_particle_field x_p,
+                                                 picasso_particle_field m_p,
+                                                 picasso_particle_field c_p,
+                                                 picasso_grid_field m_i, picasso_grid_field mu_i,
+                                                 const picasso_halo_peers* peers,
+                                                 const picasso_exec* exec);
+/* picasso_apic_g2p reading the ghost-plane velocities from the neighbours'
+ * u_i (their owned planes) instead of this rank's ghost planes: the halo
+ * gather (Picasso_FieldManager.hpp:174-181) folded into the G2P's staging of
+ * node velocities.  Tiled FP32 form only (exec->bins, F32 u_i and c_p). */
+PICASSO_API picasso_status picasso_apic_g2p_halo(const picasso_spline* sd, int64_t num_particles,
+                                                 picasso_particle_field x_p,
+                                                 picasso_grid_field u_i,
+                                                 picasso_particle_field c_p,
+                                                 const picasso_halo_peers* peers,
+                                                 const picasso_exec* exec);
+
+/* ------------------------------------------------------------------------ */
 /* Particle cell-sort                                                       */
 /* ------------------------------------------------------------------------ */
 

@@ -66,6 +66,11 @@ class Exec(C.Structure):
                 ("bins", C.POINTER(Bins)), ("overflow_count", C.c_void_p)]
 
 
+class HaloPeers(C.Structure):
+    _fields_ = [("lo_end", C.c_int32), ("hi_begin", C.c_int32), ("lo_shift", C.c_int32),
+                ("hi_shift", C.c_int32), ("lo", C.c_void_p * 2), ("hi", C.c_void_p * 2)]
+
+
 class GridUpdateParams(C.Structure):
     _fields_ = [("dt", C.c_double), ("gravity", C.c_double * 3), ("mass_threshold", C.c_double),
                 ("wall", (C.c_int32 * 2) * 3), ("wall_width", C.c_int32)]
@@ -119,6 +124,12 @@ SIGNATURES = [
     ("picasso_grid_update", C.c_int,
      [C.POINTER(Mesh), GridField, GridField, GridField, C.POINTER(GridUpdateParams), GridField,
       GridField, C.POINTER(Exec)]),
+    ("picasso_apic_p2g_halo", C.c_int,
+     [C.POINTER(Spline), C.c_int64, ParticleField, ParticleField, ParticleField, GridField,
+      GridField, C.POINTER(HaloPeers), C.POINTER(Exec)]),
+    ("picasso_apic_g2p_halo", C.c_int,
+     [C.POINTER(Spline), C.c_int64, ParticleField, GridField, ParticleField,
+      C.POINTER(HaloPeers), C.POINTER(Exec)]),
     ("picasso_apic_p2g_update_workspace", C.c_int, [C.POINTER(Bins), C.POINTER(C.c_int64)]),
     ("picasso_apic_p2g_update", C.c_int,
      [C.POINTER(Spline), C.c_int64, ParticleField, ParticleField, ParticleField, GridField,

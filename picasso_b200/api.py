@@ -297,15 +297,25 @@ class APIC:
 
     @staticmethod
     def p2g(m_p, c_p, m_i, mu_i, sd, stream=None, error_count=None, bins=None,
-            overflow_count=None):
+            overflow_count=None, peers=None):
         """APIC::p2g(m_p, c_p, m_i, mu_i, sd): adds mass and momentum into the
         grid (zero them first for the GridOperator semantics).
         `overflow_count` (int32 CUDA tensor): fixed-point grids add the
-        number of contributions out of the 64-bit range to it."""
+        number of contributions out of the 64-bit range to it.
+        `peers` (HaloPeers, e.g. SlabDecomposition.halo_peers): contributions
+        to ghost-plane nodes go straight into the neighbours' grids
+        (picasso_apic_p2g_halo; tiled precision form only)."""
         ncomp = c_p.shape[2]
         _check_grid_extent(m_i, sd.desc.mesh)
         _check_grid_extent(mu_i, sd.desc.mesh)
         ex = _exec(stream, error_count, bins, overflow_count)
+        if peers is not None:
+            check(_lib().picasso_apic_p2g_halo(C.byref(sd.desc), sd.num_particles,
+                                               particle_field(sd.x), particle_field(m_p),
+                                               particle_field(c_p), grid_field(m_i),
+                                               grid_field(mu_i), C.byref(peers),
+                                               C.byref(ex.desc)), "APIC::p2g (halo)")
+            return
         check(_lib().picasso_apic_p2g(C.byref(sd.desc), sd.num_particles, ncomp,
                                       particle_field(sd.x), particle_field(m_p),
                                       particle_field(c_p), grid_field(m_i), grid_field(mu_i),
@@ -339,11 +349,19 @@ class APIC:
             "APIC::p2g_update")
 
     @staticmethod
-    def g2p(u_i, c_p, sd, stream=None, error_count=None, bins=None):
-        """APIC::g2p(u_i, c_p, sd): overwrites c_p (4 x ncomp per particle)."""
+    def g2p(u_i, c_p, sd, stream=None, error_count=None, bins=None, peers=None):
+        """APIC::g2p(u_i, c_p, sd): overwrites c_p (4 x ncomp per particle).
+        `peers`: ghost-plane velocities are read from the neighbours' u_i
+        (picasso_apic_g2p_halo; tiled precision form only)."""
         ncomp = c_p.shape[2]
         _check_grid_extent(u_i, sd.desc.mesh)
         ex = _exec(stream, error_count, bins)
+        if peers is not None:
+            check(_lib().picasso_apic_g2p_halo(C.byref(sd.desc), sd.num_particles,
+                                               particle_field(sd.x), grid_field(u_i),
+                                               particle_field(c_p), C.byref(peers),
+                                               C.byref(ex.desc)), "APIC::g2p (halo)")
+            return
         check(_lib().picasso_apic_g2p(C.byref(sd.desc), sd.num_particles, ncomp,
                                       particle_field(sd.x), grid_field(u_i), particle_field(c_p),
                                       C.byref(ex.desc)), "APIC::g2p")

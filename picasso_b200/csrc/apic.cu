@@ -123,15 +123,17 @@ picasso_status apic_g2p_plain(const MeshP& mp, int order, int stag, int ncomp, b
 
 // Tiled kernels for binned particles (tiled.cu).
 struct FusedUpdate;
+struct HaloPeers;
 picasso_status apic_p2g_tiled(const MeshP& mp, int order, int ncomp, Form form, int64_t n,
                               const PField& x, const PField& m, const PField& c, const GField& gm,
                               const GField& gmu, const picasso_bins& bins, int* err,
                               cudaStream_t st, bool* handled, const FusedUpdate* fu = nullptr,
-                              int stag = -1);
+                              int stag = -1, const HaloPeers* hp = nullptr);
 picasso_status apic_g2p_tiled(const MeshP& mp, int order, int ncomp, bool f32, int64_t n,
                               const PField& x, const GField& u, const PField& c,
                               const picasso_bins& bins, int* err, const Advect* adv,
-                              cudaStream_t st, bool* handled, int stag = -1);
+                              cudaStream_t st, bool* handled, int stag = -1,
+                              const HaloPeers* hp = nullptr);
 
 }  // namespace pb
 

@@ -507,6 +507,8 @@ picasso_status make_instance(const picasso_batch_instance& in, bool f32, BInst* 
     // element-wise flush: in the fused launch the next phase's items read the
     // accumulators once the P2G items have counted themselves done
     I->p2g.bulk_flush = 0;
+    I->p2g.hp = HaloPeers{};
+    I->g2p.hp = HaloPeers{};
     I->g2p.mp = mp;
     I->g2p.tp = tp;
     I->g2p.x = I->p2g.x;

@@ -326,7 +326,8 @@ static const float* bins_records(const picasso_bins& bins)
 picasso_status apic_p2g_tiled(const MeshP& mp, int order, int ncomp, Form form, int64_t n,
                               const PField& x, const PField& m, const PField& c, const GField& gm,
                               const GField& gmu, const picasso_bins& bins, int* err,
-                              cudaStream_t st, bool* handled, const FusedUpdate* fu, int stag)
+                              cudaStream_t st, bool* handled, const FusedUpdate* fu, int stag,
+                              const HaloPeers* hp)
 {
     *handled = false;
     if (form != Form::F32Fixed || ncomp != 3 || !packed_x(x) || !packed_m(m) || !packed_c(c))
@@ -351,8 +352,10 @@ picasso_status apic_p2g_tiled(const MeshP& mp, int order, int ncomp, Form form, 
     A.scale_m = ldexpf(1.f, gm.fixed_bits);
     A.scale_mu = ldexpf(1.f, gmu.fixed_bits);
     A.err = err;
-    // the fused update counts its arrivals after element-wise reductions
-    A.bulk_flush = !sg && !fu && packed_accumulator(gm, gmu);
+    A.hp = hp ? *hp : HaloPeers{};
+    // the fused update counts its arrivals after element-wise reductions; a
+    // neighbour's rows take element-wise reductions too
+    A.bulk_flush = !sg && !fu && !A.hp.on && packed_accumulator(gm, gmu);
 #define PB_CASE(O, L, S)                                                                \
     if (order == O && lpp == L && sg == S)                                              \
         return rec ? launch_p2g_tiled<O, L, true, S>(A, fu, n, st)                      \
@@ -382,7 +385,7 @@ static picasso_status launch_g2p_order(const G2PArgs& A, int64_t n, cudaStream_t
 picasso_status apic_g2p_tiled(const MeshP& mp, int order, int ncomp, bool f32, int64_t n,
                               const PField& x, const GField& u, const PField& c,
                               const picasso_bins& bins, int* err, const Advect* adv,
-                              cudaStream_t st, bool* handled, int stag)
+                              cudaStream_t st, bool* handled, int stag, const HaloPeers* hp)
 {
     *handled = false;
     if (!f32 || ncomp != 3 || !packed_x(x) || !packed_c(c)) return PICASSO_OK;
@@ -400,6 +403,7 @@ picasso_status apic_g2p_tiled(const MeshP& mp, int order, int ncomp, bool f32, i
     A.err = err;
     A.x_out = adv ? reinterpret_cast<double*>(x.data) : nullptr;
     A.adv = adv ? *adv : Advect{};
+    A.hp = hp ? *hp : HaloPeers{};
     // the advection needs the positions; without it the records replace them
     A.rec = adv ? nullptr : reinterpret_cast<const float4*>(bins_records(bins));
     if (order == 1) return launch_g2p_order<1>(A, n, st, adv != nullptr, stag >= 0);
@@ -423,6 +427,93 @@ extern "C" picasso_status picasso_apic_p2g_update_workspace(const picasso_bins* 
     }
     *bytes = nt * 8 * (int64_t)sizeof(uint32_t);
     return PICASSO_OK;
+}
+
+// Halo peers of the ABI in the kernels' form; false if they do not describe
+// neighbour slabs of this (x-non-periodic) mesh.
+static bool make_halo_peers(const picasso_halo_peers* p, const MeshP& mp, int nfields,
+                            HaloPeers* hp)
+{
+    if (!p || mp.periodic[0]) return false;
+    if (p->lo_end < 0 || p->hi_begin > mp.ext[0] || p->lo_end > p->hi_begin) return false;
+    *hp = HaloPeers{};
+    hp->on = 1;
+    hp->lo_end = p->lo_end;
+    hp->hi_begin = p->hi_begin;
+    hp->lo_shift = p->lo_shift;
+    hp->hi_shift = p->hi_shift;
+    for (int f = 0; f < nfields; ++f) {
+        if ((p->lo_end > 0 && !p->lo[f]) || (p->hi_begin < mp.ext[0] && !p->hi[f])) return false;
+        hp->lo[f] = static_cast<char*>(p->lo[f]);
+        hp->hi[f] = static_cast<char*>(p->hi[f]);
+    }
+    return true;
+}
+
+extern "C" picasso_status picasso_apic_p2g_halo(const picasso_spline* sd, int64_t num_particles,
+                                                picasso_particle_field x_p,
+                                                picasso_particle_field m_p,
+                                                picasso_particle_field c_p,
+                                                picasso_grid_field m_i, picasso_grid_field mu_i,
+                                                const picasso_halo_peers* peers,
+                                                const picasso_exec* exec)
+{
+    MeshP mp;
+    picasso_status st = make_mesh(sd, &mp);
+    if (st) return st;
+    if (num_particles < 0 || !peers) return PICASSO_ERR_INVALID_ARGUMENT;
+    if ((st = validate_pfield(num_particles, x_p, PICASSO_F64))) return st;
+    if ((st = validate_pfield(num_particles, m_p, PICASSO_F64, PICASSO_F32))) return st;
+    if ((st = validate_pfield(num_particles, c_p, m_p.dtype))) return st;
+    if ((st = validate_gfield(m_i, PICASSO_F64, PICASSO_I64_FIXED))) return st;
+    if ((st = validate_gfield(mu_i, m_i.dtype))) return st;
+    if (sd->location != PICASSO_NODE || m_p.dtype != PICASSO_F32 ||
+        m_i.dtype != PICASSO_I64_FIXED || !exec || !exec->bins)
+        return PICASSO_ERR_UNSUPPORTED;
+    if (exec->bins->order != sd->order || exec->bins->location != sd->location)
+        return PICASSO_ERR_INVALID_ARGUMENT;
+    HaloPeers hp;
+    if (!make_halo_peers(peers, mp, 2, &hp)) return PICASSO_ERR_INVALID_ARGUMENT;
+    if (num_particles == 0) return PICASSO_OK;
+    const PField x = make_pfield(x_p), m = make_pfield(m_p), c = make_pfield(c_p);
+    GField gm = make_gfield(m_i), gmu = make_gfield(mu_i);
+    gm.overflow = gmu.overflow = exec->overflow_count;
+    bool handled = false;
+    st = apic_p2g_tiled(mp, sd->order, 3, Form::F32Fixed, num_particles, x, m, c, gm, gmu,
+                        *exec->bins, exec->error_count, stream_of(exec), &handled, nullptr, -1,
+                        &hp);
+    if (st) return st;
+    return handled ? PICASSO_OK : PICASSO_ERR_UNSUPPORTED;
+}
+
+extern "C" picasso_status picasso_apic_g2p_halo(const picasso_spline* sd, int64_t num_particles,
+                                                picasso_particle_field x_p,
+                                                picasso_grid_field u_i,
+                                                picasso_particle_field c_p,
+                                                const picasso_halo_peers* peers,
+                                                const picasso_exec* exec)
+{
+    MeshP mp;
+    picasso_status st = make_mesh(sd, &mp);
+    if (st) return st;
+    if (num_particles < 0 || !peers) return PICASSO_ERR_INVALID_ARGUMENT;
+    if ((st = validate_pfield(num_particles, x_p, PICASSO_F64))) return st;
+    if ((st = validate_gfield(u_i, PICASSO_F64, PICASSO_F32))) return st;
+    if ((st = validate_pfield(num_particles, c_p, u_i.dtype))) return st;
+    if (sd->location != PICASSO_NODE || u_i.dtype != PICASSO_F32 || !exec || !exec->bins)
+        return PICASSO_ERR_UNSUPPORTED;
+    if (exec->bins->order != sd->order || exec->bins->location != sd->location)
+        return PICASSO_ERR_INVALID_ARGUMENT;
+    HaloPeers hp;
+    if (!make_halo_peers(peers, mp, 1, &hp)) return PICASSO_ERR_INVALID_ARGUMENT;
+    if (num_particles == 0) return PICASSO_OK;
+    const PField x = make_pfield(x_p), c = make_pfield(c_p);
+    const GField u = make_gfield(u_i);
+    bool handled = false;
+    st = apic_g2p_tiled(mp, sd->order, 3, true, num_particles, x, u, c, *exec->bins,
+                        exec->error_count, nullptr, stream_of(exec), &handled, -1, &hp);
+    if (st) return st;
+    return handled ? PICASSO_OK : PICASSO_ERR_UNSUPPORTED;
 }
 
 extern "C" picasso_status picasso_apic_p2g_update(
@@ -487,7 +578,7 @@ extern "C" picasso_status picasso_apic_p2g_update(
     gm.overflow = gmu.overflow = exec->overflow_count;
     bool handled = false;
     st = apic_p2g_tiled(mp, sd->order, 3, Form::F32Fixed, num_particles, x, m, c, gm, gmu, *bins,
-                        exec->error_count, s, &handled, &F, -1);
+                        exec->error_count, s, &handled, &F, -1, nullptr);
     if (st || handled) return st;
     // the tiled kernel does not take these particles (layout, tile size):
     // the fill of u above is overwritten by the separate update

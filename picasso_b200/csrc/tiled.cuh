@@ -66,6 +66,39 @@ struct TileP {
     const uint32_t* items;  // tile work-item prefix (ntiles + 1)
 };
 
+// Neighbour grids of a slab decomposition along x: the local x-planes below
+// lo_end are the lower neighbour's planes (index + lo_shift there), those
+// from hi_begin on the upper neighbour's (index + hi_shift); the neighbours'
+// grids have the local strides.  P2G adds the sums of those nodes into the
+// neighbour's grid (lo[0] / hi[0]: mass, [1]: momentum) and G2P reads their
+// velocities from it ([0]): the halo exchange happens inside the transfers,
+// through peer memory when the neighbour is another GPU.
+struct HaloPeers {
+    int on;
+    int lo_end, hi_begin;
+    int lo_shift, hi_shift;
+    char* lo[2];
+    char* hi[2];
+};
+
+// Grid base holding local x-plane gi (own, or a neighbour's field f) and the
+// plane's index there.
+__device__ __forceinline__ char* halo_route(const HaloPeers& hp, int f, char* own, int gi, int& gx)
+{
+    gx = gi;
+    if (hp.on) {
+        if (gi < hp.lo_end) {
+            gx = gi + hp.lo_shift;
+            return hp.lo[f];
+        }
+        if (gi >= hp.hi_begin) {
+            gx = gi + hp.hi_shift;
+            return hp.hi[f];
+        }
+    }
+    return own;
+}
+
 // Per-call (per-instance) arguments of the tiled kernels.
 struct P2GArgs {
     MeshP mp;
@@ -84,6 +117,7 @@ struct P2GArgs {
     // consecutive 64-bit words, 16-byte aligned): the item's flush adds whole
     // k-rows with bulk reductions (flush_rows_bulk)
     int bulk_flush;
+    HaloPeers hp;
 };
 
 struct G2PArgs {
@@ -97,6 +131,7 @@ struct G2PArgs {
     int* err;
     double* x_out;  // G2P with advection: positions updated in place (= x)
     Advect adv;
+    HaloPeers hp;
 };
 
 __device__ __forceinline__ int bin_of(const MeshP& mp, const TileP& tp, int d, int s0)
@@ -925,15 +960,21 @@ __device__ void p2g_item(const P2GArgs& A, int64_t t, int64_t a, int64_t b, floa
             const int gi = node_global(mp, tp, 0, ob[0], i);
             const int gj = node_global(mp, tp, 1, ob[1], j);
             const int gk = node_global(mp, tp, 2, ob[2], k);
+            // this rank's grids, or the neighbour's that owns plane gi
+            int gx_m, gx_mu;
+            char* bm = halo_route(A.hp, 0, A.gm.data, gi, gx_m);
+            char* bmu = halo_route(A.hp, 1, A.gmu.data, gi, gx_mu);
 #pragma unroll
             for (int f = 0; f < C::NF; ++f) {
                 const TileVal v = tile[f * tp.P + idx];
                 if (v != TileVal(0)) {
                     const long long q = to_fixed(
                         f == 0 ? A.gm : A.gmu, v * (TileVal)(f == 0 ? A.scale_m : A.scale_mu));
-                    unsigned long long* dst = reinterpret_cast<unsigned long long*>(
-                        f == 0 ? A.gm.ptr<long long>(gi, gj, gk, 0)
-                               : A.gmu.ptr<long long>(gi, gj, gk, STAG ? 0 : f - 1));
+                    unsigned long long* dst =
+                        f == 0 ? reinterpret_cast<unsigned long long*>(bm) +
+                                     A.gm.index(gx_m, gj, gk, 0)
+                               : reinterpret_cast<unsigned long long*>(bmu) +
+                                     A.gmu.index(gx_mu, gj, gk, STAG ? 0 : f - 1);
                     atomicAdd(dst, (unsigned long long)q);
                 }
             }
@@ -1171,10 +1212,13 @@ __device__ void g2p_item(const G2PArgs& A, int64_t t, int64_t a, int64_t b, floa
                             (mp.periodic[2] || gk < mp.ext[2]);
         float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
         if (inside) {  // through L2: the batched kernel writes u_i in the same launch
-            v.x = __ldcg(A.u.ptr<float>(gi, gj, gk, 0));
+            int gx;
+            const float* ub =
+                reinterpret_cast<const float*>(halo_route(A.hp, 0, A.u.data, gi, gx));
+            v.x = __ldcg(ub + A.u.index(gx, gj, gk, 0));
             if (!STAG) {
-                v.y = __ldcg(A.u.ptr<float>(gi, gj, gk, 1));
-                v.z = __ldcg(A.u.ptr<float>(gi, gj, gk, 2));
+                v.y = __ldcg(ub + A.u.index(gx, gj, gk, 1));
+                v.z = __ldcg(ub + A.u.index(gx, gj, gk, 2));
             }
         }
         tile[(i * tp.NT[1] + j) * tp.NT[2] + k] = v;

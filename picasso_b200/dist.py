@@ -26,6 +26,13 @@ per GPU with torch.distributed (NCCL between GPUs, gloo on the CPU):
 * ``migrate`` (after the positions moved, by less than one slab): particles
   whose x left the owned range go to the neighbour that owns them; x is
   wrapped into the global box.
+* ``halo_peers`` / ``map_peer_grids``: the device form of the two exchanges.
+  With the neighbours' grids mapped into this process (CUDA IPC with peer
+  access between GPUs), the tiled P2G adds its ghost-plane sums straight into
+  the neighbour's owned planes and the tiled G2P reads its ghost velocities
+  from the neighbour's owned planes (picasso_apic_p2g_halo /
+  picasso_apic_g2p_halo): no ghost planes are sent, and the only host step
+  left is a barrier after each transfer.
 
 Every rank takes the same collective steps in the same order.  Two phases per
 exchange (towards +x, then towards -x) keep the messages of two ranks that
@@ -118,6 +125,51 @@ class SlabDecomposition:
             lo, ln = self.low[d], self.length[d]
             x[:, d] = lo + torch.remainder(x[:, d] - lo, ln)
         return x
+
+    # -- exchanges inside the transfers ----------------------------------------
+    def halo_peers(self, lower, upper):
+        """HaloPeers for APIC.p2g / APIC.g2p(peers=...): `lower` and `upper`
+        are the neighbours' grids of the same shapes as this rank's -- (m_i,
+        mu_i) for P2G, u_i for G2P -- as tensors (or FixedGrid) addressable
+        from this device: the neighbouring slabs' arrays on this GPU, or the
+        ones map_peer_grids returns.  Local plane p < halo is the lower
+        neighbour's plane p + own(lower), plane p >= halo + own the upper
+        neighbour's plane p - own."""
+        if self.world == 1:
+            raise ValueError("a single slab is periodic along x and has no neighbours")
+
+        def ptrs(g):
+            gs = g if isinstance(g, (tuple, list)) else (g,)
+            return [(x.raw if hasattr(x, "raw") else x).data_ptr() for x in gs] + [None]
+
+        p = _abi.HaloPeers()
+        p.lo_end = self.halo
+        p.hi_begin = self.halo + self.own
+        p.lo_shift = self.sizes[self.lower]
+        p.hi_shift = -self.own
+        lo, hi = ptrs(lower), ptrs(upper)
+        for f in range(2):
+            p.lo[f] = lo[f]
+            p.hi[f] = hi[f]
+        return p
+
+    def map_peer_grids(self, *grids):
+        """Maps the neighbours' copies of `grids` into this process: every rank
+        calls it with its own grids (same shapes and order; FixedGrid or
+        tensors) and gets (lower, upper), lists of tensors over the lower and
+        upper neighbours' memory (CUDA IPC handles exchanged through the
+        process group; peer access between GPUs).  The grids must stay
+        allocated while the mapping is used."""
+        from torch.multiprocessing.reductions import reduce_tensor
+        raws = [g.raw if hasattr(g, "raw") else g for g in grids]
+        # per grid: the IPC handle of its storage and the view's geometry
+        mine = [reduce_tensor(r) for r in raws]
+        everyone = [None] * self.world
+        tdist.all_gather_object(everyone, mine, group=self.group)
+
+        def load(r):
+            return [fn(*args) for fn, args in everyone[r]]
+        return load(self.lower), load(self.upper)
 
     # -- exchanges ------------------------------------------------------------
     def _shift(self, send, to, recv, frm):
