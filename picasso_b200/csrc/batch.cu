@@ -276,7 +276,7 @@ batch_kernel(BatchDev B, uint32_t qlo, uint32_t qhi, int slot)
 {
     constexpr int NT = BatchShape<F32, PMASK, VAR>::threads;
     extern __shared__ __align__(16) float smem[];
-    __shared__ int stage_base[kStageLanes];
+    __shared__ int stage_base[kStageBases];
     __shared__ uint32_t s_item;
     __shared__ __align__(16) P2GArgs s_p2g;
     __shared__ __align__(16) G2PArgs s_g2p;

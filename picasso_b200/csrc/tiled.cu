@@ -24,7 +24,7 @@ __global__ void __launch_bounds__(32, (P2GOccupancy<ORDER, LPP>::value))
 p2g_tiled_kernel(P2GArgs A, FusedUpdate F, int64_t n)
 {
     extern __shared__ __align__(16) float smem[];
-    __shared__ int stage_base[kStageLanes];
+    __shared__ int stage_base[kStageBases];
     if (blockIdx.x == 0 && threadIdx.x == 0 && A.err) {
         const int64_t n_valid = __ldg(A.tp.off + A.tp.ntiles);
         if (n > n_valid) atomicAdd(A.err, (int)(n - n_valid));

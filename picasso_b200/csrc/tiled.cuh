@@ -39,7 +39,8 @@
 
 namespace pb {
 
-constexpr int kStageLanes = 8;  // lanes staged per merge round
+constexpr int kStageLanes = 8;   // lanes staged per full merge round
+constexpr int kStageBases = 32;  // stage_base entries (k-plane merges stage every lane at once)
 constexpr unsigned kFull = 0xFFFFFFFFu;
 
 // Element type of the P2G node tile that sums the lanes' FP32 partials.
@@ -313,7 +314,10 @@ struct P2GCfg {
     // loads: 256^3 8 ppc, tile (4, 4, 8): depth 4 14.6 ms, 6 14.7, 10 15.7).
     static constexpr int DEPTH = LPP == 1 ? 4 : (LPP == 2 ? 8 : (ORDER == 3 ? 4 : 10));
     static constexpr int STAGE_OFF = DEPTH * RING;
-    static constexpr int TILE_OFF = STAGE_OFF + kStageLanes * SS;
+    // staging area: kStageLanes full stencils, or the first k-plane of every
+    // lane (used one after the other)
+    static constexpr int STAGE_FLOATS = 32 * PS > kStageLanes * SS ? 32 * PS : kStageLanes * SS;
+    static constexpr int TILE_OFF = STAGE_OFF + STAGE_FLOATS;
     static_assert(LPP == 1 || LPP == 2 || LPP == 4, "1, 2 or 4 lanes per particle");
     static_assert(F >= 1, "at least one field per lane");
 };
@@ -546,28 +550,47 @@ struct MergePlan {
     }
 };
 
-// The warp adds the values of `nstage` staged lanes (slot q: stage + q SLOT,
-// its base in stage_base[q]) into the node tile: lane l adds value l + 32 r
-// of each slot at tile offset base + off[r], slot after slot (a fixed order,
-// so the tile sums are reproducible).
-template <int NR, int SLOT, int LPP>
-__device__ __forceinline__ void add_staged(int nstage, const float* stage, const int* stage_base,
-                                           const int (&off)[NR], unsigned valid, int fstride,
-                                           TileVal* tile, int lane)
+// The warp adds staged values into the node tile: lane l adds value l + 32 r
+// of each staged slot at tile offset base + off[r], slot after slot in a
+// fixed order (so the tile sums are reproducible): slots 0 .. n - 1 (LANES
+// false, n = `slots`) or the set bits of `slots`, lowest first (LANES true,
+// not empty).  The next slot's base and values are read before this slot's
+// tile updates, so only the tile read-add-write is on the dependency chain.
+template <int NR, int SLOT, int LPP, bool LANES>
+__device__ __forceinline__ void add_staged(unsigned slots, const float* stage,
+                                           const int* stage_base, const int (&off)[NR],
+                                           unsigned valid, int fstride, TileVal* tile, int lane)
 {
-    for (int q = 0; q < nstage; ++q) {
-        const float* st = stage + q * SLOT;
-        const int sb = stage_base[q];
+    int q = LANES ? __ffs(slots) - 1 : 0;
+    unsigned rest = LANES ? slots & (slots - 1u) : slots - 1u;  // LANES false: slots left
+    int sb = stage_base[q];
+    float v[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r)
+        v[r] = ((valid >> r) & 1u) ? stage[q * SLOT + lane + 32 * r] : 0.f;
+    for (;;) {
+        const int qn = rest ? (LANES ? __ffs(rest) - 1 : q + 1) : q;
+        const int sbn = stage_base[qn];
+        float vn[NR];
+#pragma unroll
+        for (int r = 0; r < NR; ++r)
+            vn[r] = ((valid >> r) & 1u) ? stage[qn * SLOT + lane + 32 * r] : 0.f;
         const int base = (sb & 0x0FFFFFFF) + (LPP > 1 ? (sb >> 28) * fstride : 0);
 #pragma unroll
         for (int r = 0; r < NR; ++r)
-            if ((valid >> r) & 1u) tile[base + off[r]] += st[lane + 32 * r];
+            if ((valid >> r) & 1u) tile[base + off[r]] += v[r];
         __syncwarp();
+        if (!rest) break;
+        rest = LANES ? rest & (rest - 1u) : rest - 1u;
+        q = qn;
+        sb = sbn;
+#pragma unroll
+        for (int r = 0; r < NR; ++r) v[r] = vn[r];
     }
 }
 
 // Lanes in `mask` hand their partial sums to the warp's node tile in lane
-// order; their accumulators are zeroed.
+// order (rounds of at most kStageLanes lanes); their accumulators are zeroed.
 template <int ORDER, int LPP, bool STAG>
 __device__ __forceinline__ void merge_partials(unsigned mask, P2GAcc<ORDER, LPP, STAG>& acc,
                                                int cur_base,
@@ -595,41 +618,29 @@ __device__ __forceinline__ void merge_partials(unsigned mask, P2GAcc<ORDER, LPP,
             acc.zero();
         }
         __syncwarp();
-        add_staged<C::R, C::SS, LPP>(__popc(batch), stage, stage_base, plan.moff, plan.valid,
-                                     plan.fstride, tile, lane);
+        add_staged<C::R, C::SS, LPP, false>(__popc(batch), stage, stage_base, plan.moff,
+                                            plan.valid, plan.fstride, tile, lane);
     }
 }
 
 // Lanes in `mask` (whose bin moved one step along k) hand the first k-plane
-// of their sums to the node tile in lane order and shift the rest down.
+// of their sums to the node tile and shift the rest down: every lane of the
+// mask stages its plane in its own slot and shifts (one pass for the warp),
+// then the warp adds the planes in lane order.
 template <int ORDER, int LPP, bool STAG>
 __device__ __forceinline__ void merge_plane(unsigned mask, P2GAcc<ORDER, LPP, STAG>& acc,
                                             int cur_base, const MergePlan<ORDER, LPP, STAG>& plan,
                                             TileVal* tile, float* stage, int* stage_base, int lane)
 {
     using C = P2GCfg<ORDER, LPP, false, STAG>;
-    while (mask) {
-        unsigned batch = mask;
-        if (__popc(mask) > kStageLanes) {
-            batch = 0;
-            unsigned mm = mask;
-#pragma unroll
-            for (int q = 0; q < kStageLanes; ++q) {
-                batch |= mm & (~mm + 1u);
-                mm &= mm - 1u;
-            }
-        }
-        mask &= ~batch;
-        if ((batch >> lane) & 1u) {
-            const int slot = __popc(batch & ((1u << lane) - 1u));
-            acc.stage_plane(stage + slot * C::PS);
-            stage_base[slot] = cur_base | ((lane % LPP) << 28);
-            acc.shift_k();
-        }
-        __syncwarp();
-        add_staged<C::RP, C::PS, LPP>(__popc(batch), stage, stage_base, plan.poff, plan.pvalid,
-                                      plan.fstride, tile, lane);
+    if ((mask >> lane) & 1u) {
+        acc.stage_plane(stage + lane * C::PS);
+        acc.shift_k();
     }
+    stage_base[lane] = cur_base | ((lane % LPP) << 28);
+    __syncwarp();
+    add_staged<C::RP, C::PS, LPP, true>(mask, stage, stage_base, plan.poff, plan.pvalid,
+                                        plan.fstride, tile, lane);
 }
 
 // Bin inside tile t of a particle from its sort key; false if the key is
