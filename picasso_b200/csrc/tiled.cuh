@@ -1290,7 +1290,7 @@ __device__ void g2p_item(const G2PArgs& A, int64_t t, int64_t a, int64_t b, floa
         //   B_p(:,q) = dx M_q + dist_q(n0) u_p
         float up[3] = {0.f, 0.f, 0.f};
         float M[3][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
-        if constexpr (K != 4) {
+        if constexpr (K != 4 || ADV) {
 #pragma unroll
             for (int i = 0; i < K; ++i) {
                 float A0[3] = {0.f, 0.f, 0.f}, A1[3] = {0.f, 0.f, 0.f}, A2[3] = {0.f, 0.f, 0.f};
@@ -1329,11 +1329,13 @@ __device__ void g2p_item(const G2PArgs& A, int64_t t, int64_t a, int64_t b, floa
                 }
             }
         } else {
-            // Cubic stencils: each sum over a knot index is one FMA chain,
-            // sum_n w_n v_n and sum_n (n - n0) w_n v_n with the factor folded into
-            // the FMA (knot_mac; KF is the first knot with n != n0): 3.88 -> 3.70 ms
-            // at 256^3 8 ppc.  For the smaller stencils the compiler already forms
-            // the same chains from the form above (bit-identical results).
+            // Cubic stencils without advection: each sum over a knot index is
+            // one FMA chain, sum_n w_n v_n and sum_n (n - n0) w_n v_n with the
+            // factor folded into the FMA (knot_mac; KF is the first knot with
+            // n != n0): 3.88 -> 3.70 ms at 256^3 8 ppc.  The advecting kernel
+            // measured slower with it (5.68 -> 5.80 ms), and for the smaller
+            // stencils the compiler already forms the same chains from the form
+            // above (bit-identical results).
             constexpr int KF = N0 == 0 ? 1 : 0;
 #pragma unroll
             for (int i = 0; i < K; ++i) {
