@@ -337,17 +337,6 @@ __host__ __device__ constexpr int p2g_warp_floats(int P)
            P2GCfg<ORDER, LPP, REC, STAG>::NF * P * kTileWords;
 }
 
-// acc + s w v for a small integer s (s = 0: acc; `first`: acc holds no term
-// yet, the result is s w v).  Called with unrolled loop indices, so the
-// branches fold at compile time and the factor -1 becomes the sign of the
-// multiply or FMA.
-__device__ __forceinline__ float knot_mac(int s, bool first, float w, float v, float acc)
-{
-    if (s == 0) return acc;
-    const float ws = s == 1 ? w : (s == -1 ? -w : (float)s * w);
-    return first ? ws * v : fmaf(ws, v, acc);
-}
-
 // p + s g for a small integer s (s = 0: p exactly).  Called with unrolled
 // loop indices, so the branch folds at compile time.
 __device__ __forceinline__ float add_steps(int s, float p, float g)
@@ -1290,87 +1279,41 @@ __device__ void g2p_item(const G2PArgs& A, int64_t t, int64_t a, int64_t b, floa
         //   B_p(:,q) = dx M_q + dist_q(n0) u_p
         float up[3] = {0.f, 0.f, 0.f};
         float M[3][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
-        if constexpr (K != 4 || ADV) {
 #pragma unroll
-            for (int i = 0; i < K; ++i) {
-                float A0[3] = {0.f, 0.f, 0.f}, A1[3] = {0.f, 0.f, 0.f}, A2[3] = {0.f, 0.f, 0.f};
+        for (int i = 0; i < K; ++i) {
+            float A0[3] = {0.f, 0.f, 0.f}, A1[3] = {0.f, 0.f, 0.f}, A2[3] = {0.f, 0.f, 0.f};
 #pragma unroll
-                for (int j = 0; j < K; ++j) {
-                    const float4* row = tile + base + (i * tp.NT[1] + j) * tp.NT[2];
-                    float S0[3] = {0.f, 0.f, 0.f}, S1[3] = {0.f, 0.f, 0.f};
+            for (int j = 0; j < K; ++j) {
+                const float4* row = tile + base + (i * tp.NT[1] + j) * tp.NT[2];
+                float S0[3] = {0.f, 0.f, 0.f}, S1[3] = {0.f, 0.f, 0.f};
 #pragma unroll
-                    for (int k = 0; k < K; ++k) {
-                        const float4 ue = row[k];
-                        const float uk[3] = {ue.x, ue.y, ue.z};
-#pragma unroll
-                        for (int d = 0; d < NU; ++d) {
-                            const float wu = sp[2].w[k] * uk[d];
-                            S0[d] += wu;
-                            S1[d] = add_steps(k - N0, S1[d], wu);
-                        }
-                    }
-                    const float wy = sp[1].w[j];
+                for (int k = 0; k < K; ++k) {
+                    const float4 ue = row[k];
+                    const float uk[3] = {ue.x, ue.y, ue.z};
 #pragma unroll
                     for (int d = 0; d < NU; ++d) {
-                        const float wS0 = wy * S0[d];
-                        A0[d] += wS0;
-                        A1[d] = add_steps(j - N0, A1[d], wS0);
-                        A2[d] = fmaf(wy, S1[d], A2[d]);
+                        const float wu = sp[2].w[k] * uk[d];
+                        S0[d] += wu;
+                        S1[d] = add_steps(k - N0, S1[d], wu);
                     }
                 }
-                const float wx = sp[0].w[i];
+                const float wy = sp[1].w[j];
 #pragma unroll
                 for (int d = 0; d < NU; ++d) {
-                    const float wA0 = wx * A0[d];
-                    up[d] += wA0;
-                    M[d][0] = add_steps(i - N0, M[d][0], wA0);
-                    M[d][1] = fmaf(wx, A1[d], M[d][1]);
-                    M[d][2] = fmaf(wx, A2[d], M[d][2]);
+                    const float wS0 = wy * S0[d];
+                    A0[d] += wS0;
+                    A1[d] = add_steps(j - N0, A1[d], wS0);
+                    A2[d] = fmaf(wy, S1[d], A2[d]);
                 }
             }
-        } else {
-            // Cubic stencils without advection: each sum over a knot index is
-            // one FMA chain, sum_n w_n v_n and sum_n (n - n0) w_n v_n with the
-            // factor folded into the FMA (knot_mac; KF is the first knot with
-            // n != n0): 3.88 -> 3.70 ms at 256^3 8 ppc.  The advecting kernel
-            // measured slower with it (5.68 -> 5.80 ms), and for the smaller
-            // stencils the compiler already forms the same chains from the form
-            // above (bit-identical results).
-            constexpr int KF = N0 == 0 ? 1 : 0;
+            const float wx = sp[0].w[i];
 #pragma unroll
-            for (int i = 0; i < K; ++i) {
-                float A0[3] = {0.f, 0.f, 0.f}, A1[3] = {0.f, 0.f, 0.f}, A2[3] = {0.f, 0.f, 0.f};
-#pragma unroll
-                for (int j = 0; j < K; ++j) {
-                    const float4* row = tile + base + (i * tp.NT[1] + j) * tp.NT[2];
-                    float S0[3] = {0.f, 0.f, 0.f}, S1[3] = {0.f, 0.f, 0.f};
-#pragma unroll
-                    for (int k = 0; k < K; ++k) {
-                        const float4 ue = row[k];
-                        const float uk[3] = {ue.x, ue.y, ue.z};
-                        const float wz = sp[2].w[k];
-#pragma unroll
-                        for (int d = 0; d < NU; ++d) {
-                            S0[d] = k == 0 ? wz * uk[d] : fmaf(wz, uk[d], S0[d]);
-                            S1[d] = knot_mac(k - N0, k == KF, wz, uk[d], S1[d]);
-                        }
-                    }
-                    const float wy = sp[1].w[j];
-#pragma unroll
-                    for (int d = 0; d < NU; ++d) {
-                        A0[d] = j == 0 ? wy * S0[d] : fmaf(wy, S0[d], A0[d]);
-                        A1[d] = knot_mac(j - N0, j == KF, wy, S0[d], A1[d]);
-                        A2[d] = j == 0 ? wy * S1[d] : fmaf(wy, S1[d], A2[d]);
-                    }
-                }
-                const float wx = sp[0].w[i];
-#pragma unroll
-                for (int d = 0; d < NU; ++d) {
-                    up[d] = i == 0 ? wx * A0[d] : fmaf(wx, A0[d], up[d]);
-                    M[d][0] = knot_mac(i - N0, i == KF, wx, A0[d], M[d][0]);
-                    M[d][1] = i == 0 ? wx * A1[d] : fmaf(wx, A1[d], M[d][1]);
-                    M[d][2] = i == 0 ? wx * A2[d] : fmaf(wx, A2[d], M[d][2]);
-                }
+            for (int d = 0; d < NU; ++d) {
+                const float wA0 = wx * A0[d];
+                up[d] += wA0;
+                M[d][0] = add_steps(i - N0, M[d][0], wA0);
+                M[d][1] = fmaf(wx, A1[d], M[d][1]);
+                M[d][2] = fmaf(wx, A2[d], M[d][2]);
             }
         }
         float B[3][3];
