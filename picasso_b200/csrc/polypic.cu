@@ -445,8 +445,10 @@ __device__ __forceinline__ void count_unsorted(const TileP& tp, int64_t n, int* 
 // is bit-identical to the plain kernel's (which adds every contribution to
 // the grid), with one grid atomic per touched node and field per item
 // instead of per particle and node.
+// Quadratic: 3 CTAs per SM (168 registers, 44 bytes of spills) instead of 2 at
+// 255 registers: 27 modes at 128^3 8 ppc 6.24 -> 5.85 ms.
 template <int ORDER, int NC>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, ORDER == 2 ? 3 : 1)
 polypic_p2g_tiled_kernel(MeshP mp, TileP tp, int64_t n, PField x, PField m, PField u, PField c,
                          GField gmu, GField gm, float dt, float scale_mu, float scale_m, int* err)
 {
