@@ -441,10 +441,10 @@ __device__ __forceinline__ void count_unsorted(const TileP& tp, int64_t n, int* 
 // 65536 contributions are exact, the hi sum is exact modulo 2^32) or on two
 // words (the low word's carries, read from the atomics' old values, added to
 // the high word), so the recombined 64-bit total equals the sum of the q
-// modulo 2^64; then the tile is added to the grid.  Integer sums do not depend on their order: the grid
-// is bit-identical to the plain kernel's (which adds every contribution to
-// the grid), with one grid atomic per touched node and field per item
-// instead of per particle and node.
+// modulo 2^64; then the tile is added to the grid.  Integer sums do not
+// depend on their order: the grid is bit-identical to the plain kernel's
+// (which adds every contribution to the grid), with one grid atomic per
+// touched node and field per item instead of per particle and node.
 // Quadratic: 3 CTAs per SM (168 registers, 44 bytes of spills) instead of 2 at
 // 255 registers: 27 modes at 128^3 8 ppc 6.24 -> 5.85 ms.
 template <int ORDER, int NC>
