@@ -318,6 +318,13 @@ struct P2GCfg {
     // lane (used one after the other)
     static constexpr int STAGE_FLOATS = 32 * PS > kStageLanes * SS ? 32 * PS : kStageLanes * SS;
     static constexpr int TILE_OFF = STAGE_OFF + STAGE_FLOATS;
+    // plane split with records, collocated: the lanes of a run evaluate the
+    // splines and affine form of the run's next LPP particles once (one
+    // particle each) and share them through a table after the node tile
+    // (p2g_item)
+    static constexpr bool SHARE = ISPLIT && REC && !STAG;
+    static constexpr int ENTRY = 28;  // floats of one particle's table entry
+    static constexpr int TABLE = SHARE ? 32 * ENTRY : 0;
     static_assert(LPP == 1 || LPP == 2 || LPP == 4, "1, 2 or 4 lanes per particle");
     static_assert(F >= 1, "at least one field per lane");
 };
@@ -334,7 +341,8 @@ template <int ORDER, int LPP, bool REC = false, bool STAG = false>
 __host__ __device__ constexpr int p2g_warp_floats(int P)
 {
     return P2GCfg<ORDER, LPP, REC, STAG>::TILE_OFF +
-           P2GCfg<ORDER, LPP, REC, STAG>::NF * P * kTileWords;
+           P2GCfg<ORDER, LPP, REC, STAG>::NF * P * kTileWords +
+           P2GCfg<ORDER, LPP, REC, STAG>::TABLE;
 }
 
 // p + s g for a small integer s (s = 0: p exactly).  Called with unrolled
@@ -372,32 +380,11 @@ struct P2GAcc {
         constexpr int N0 = C::N0;
         constexpr bool MASS0 = C::ISPLIT || LPP == 1;
         if constexpr (C::ISPLIT) {
-            // node (h, j, k): w = wx_h wy_j wz_k m
             float wx = 0.f;
 #pragma unroll
             for (int i = 0; i < K; ++i)
                 if (i == h) wx = sp[0].w[i];
-            const float wxm = wx * mass;
-            const float hs = (float)(h - N0);
-            float pi[C::F];
-#pragma unroll
-            for (int f = 1; f < C::F; ++f) pi[f] = fmaf(hs, G[f][0], E[f]);
-#pragma unroll
-            for (int j = 0; j < K; ++j) {
-                const float wij = wxm * sp[1].w[j];
-                float pij[C::F];
-#pragma unroll
-                for (int f = 1; f < C::F; ++f) pij[f] = add_steps(j - N0, pi[f], G[f][1]);
-#pragma unroll
-                for (int k = 0; k < K; ++k) {
-                    const int n = j * K + k;
-                    const float w = wij * sp[2].w[k];
-                    acc[0][n] += w;
-#pragma unroll
-                    for (int f = 1; f < C::F; ++f)
-                        acc[f][n] = fmaf(w, add_steps(k - N0, pij[f], G[f][2]), acc[f][n]);
-                }
-            }
+            add_isplit(wx, sp[1].w, sp[2].w, mass, E, G, h);
         } else {
 #pragma unroll
             for (int i = 0; i < K; ++i) {
@@ -424,6 +411,37 @@ struct P2GAcc {
                         }
                     }
                 }
+            }
+        }
+    }
+
+    // Plane split: the lane's i-plane h, x-weight wx = w_x[h]; node (h, j, k)
+    // receives w = wx m wy_j wz_k.
+    __device__ __forceinline__ void add_isplit(float wx, const float* wy, const float* wz,
+                                               float mass, const float E[C::F],
+                                               const float G[C::F][3], int h)
+    {
+        constexpr int K = C::K;
+        constexpr int N0 = C::N0;
+        const float wxm = wx * mass;
+        const float hs = (float)(h - N0);
+        float pi[C::F];
+#pragma unroll
+        for (int f = 1; f < C::F; ++f) pi[f] = fmaf(hs, G[f][0], E[f]);
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            const float wij = wxm * wy[j];
+            float pij[C::F];
+#pragma unroll
+            for (int f = 1; f < C::F; ++f) pij[f] = add_steps(j - N0, pi[f], G[f][1]);
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                const int n = j * K + k;
+                const float w = wij * wz[k];
+                acc[0][n] += w;
+#pragma unroll
+                for (int f = 1; f < C::F; ++f)
+                    acc[f][n] = fmaf(w, add_steps(k - N0, pij[f], G[f][2]), acc[f][n]);
             }
         }
     }
@@ -915,6 +933,88 @@ __device__ void p2g_item(const P2GArgs& A, int64_t t, int64_t a, int64_t b, floa
     Acc acc;
     acc.zero();
     int cur = -1, cur_base = 0;
+    if constexpr (C::SHARE) {
+        // Groups of LPP steps: lane h of a run evaluates particle s0 + h of
+        // the run (record, splines, bin, affine form) and writes it to the
+        // table; in sub-step q the run's lanes read entry (q, run).  Entries
+        // are sub-step-major so that the 8 runs' entries of one sub-step fall
+        // on different banks.  The ring holds one group (DEPTH == LPP): the
+        // next group's records are issued once the entries are written and
+        // arrive during the sub-steps.  Same arithmetic as the loop below.
+        static_assert(C::DEPTH == LPP, "one group in the ring");
+        float* table = warp_smem + C::TILE_OFF + C::NF * tp.P * kTileWords;
+        issue(C::DEPTH - 1);  // steps 0 .. DEPTH - 2 are in flight
+        for (int s0 = 0; s0 < U; s0 += LPP) {
+            cp_async_wait<0>();  // the group's records have landed
+            __syncwarp();        // ... for every lane of each run
+            {
+                const int q = s0 + h;
+                Spline1D<ORDER, float> sp[3];
+                int lb[3] = {0, 0, 0};
+                bool ok = false;
+                float cp[12], mass = 0.f;
+#pragma unroll
+                for (int v = 0; v < 12; ++v) cp[v] = 0.f;
+#pragma unroll
+                for (int d = 0; d < 3; ++d)
+#pragma unroll
+                    for (int n = 0; n < K; ++n) sp[d].w[n] = sp[d].d[n] = 0.f;
+                if (q < cnt) {
+                    const float4 r = *reinterpret_cast<const float4*>(slot(q) + C::RING_X + run * 4);
+                    ok = locate_record<ORDER>(mp, tp, t, r, sp, lb);
+                    // a particle out of the item's rows is skipped like one of
+                    // another tile
+                    ok = ok && lb[0] >= i_lo && lb[0] <= i_hi;
+                    if (!ok && A.err) atomicAdd(A.err, 1);
+                    read_c(q, cp, mass);
+                }
+                float E[C::F], G[C::F][3];
+                centre_form(cp, sp, E, G);
+                float4* e = reinterpret_cast<float4*>(table + (h * C::RUNS + run) * C::ENTRY);
+                e[0] = make_float4(sp[0].w[0], sp[0].w[1], sp[0].w[2], sp[0].w[3]);
+                e[1] = make_float4(sp[1].w[0], sp[1].w[1], sp[1].w[2], sp[1].w[3]);
+                e[2] = make_float4(sp[2].w[0], sp[2].w[1], sp[2].w[2], sp[2].w[3]);
+                e[3] = make_float4(mass, E[1], E[2], E[3]);
+                e[4] = make_float4(G[1][0], G[1][1], G[1][2], G[2][0]);
+                e[5] = make_float4(G[2][1], G[2][2], G[3][0], G[3][1]);
+                const int lbin = ok ? (lb[0] * tp.T[1] + lb[1]) * tp.T[2] + lb[2] : -1;
+                e[6] = make_float4(G[3][2], __int_as_float(lbin),
+                                   __int_as_float(lb[0] * tp.SI + lb[1] * tp.SJ + lb[2]),
+                                   __int_as_float(lb[2]));
+            }
+            __syncwarp();  // entries written, the group's ring slots read
+#pragma unroll
+            for (int q = 0; q < LPP; ++q) issue(s0 + LPP + q);
+            for (int q = 0; q < LPP; ++q) {
+                const float* ef = table + (q * C::RUNS + run) * C::ENTRY;
+                const float4* e = reinterpret_cast<const float4*>(ef);
+                const float wx = ef[h];
+                const float4 wy4 = e[1], wz4 = e[2], me = e[3], g0 = e[4], g1 = e[5], g2 = e[6];
+                const int lbin = __float_as_int(g2.y);
+                const bool ok = lbin >= 0;
+                const bool chg = ok && cur >= 0 && lbin != cur;
+                const bool kstep = chg && lbin == cur + 1 && __float_as_int(g2.w) != 0;
+                const unsigned pm = __ballot_sync(kFull, kstep);
+                const unsigned fm = __ballot_sync(kFull, chg && !kstep);
+                if (pm) merge_plane(pm, acc, cur_base, plan, tile, stage, stage_base, lane);
+                if (fm) merge_partials(fm, acc, cur_base, plan, tile, stage, stage_base, lane);
+                if (ok) {
+                    if (lbin != cur) {
+                        cur = lbin;
+                        cur_base = __float_as_int(g2.z);
+                    }
+                    const float wy[4] = {wy4.x, wy4.y, wy4.z, wy4.w};
+                    const float wz[4] = {wz4.x, wz4.y, wz4.z, wz4.w};
+                    const float E[C::F] = {1.f, me.y, me.z, me.w};
+                    const float G[C::F][3] = {{0.f, 0.f, 0.f},
+                                              {g0.x, g0.y, g0.z},
+                                              {g0.w, g1.x, g1.y},
+                                              {g1.z, g1.w, g2.x}};
+                    acc.add_isplit(wx, wy, wz, me.x, E, G, h);
+                }
+            }
+        }
+    } else
     for (int s = 0; s < U; ++s) {
         __syncwarp();  // no lane still reads the slot refilled next
         issue(s + C::DEPTH - 1);
