@@ -324,7 +324,8 @@ struct P2GCfg {
     // (p2g_item)
     static constexpr bool SHARE = ISPLIT && REC && !STAG;
     static constexpr int ENTRY = 28;  // floats of one particle's table entry
-    static constexpr int TABLE = SHARE ? 32 * ENTRY : 0;
+    // entries of sub-step q start 8 q floats later (bank skew, p2g_item)
+    static constexpr int TABLE = SHARE ? 32 * ENTRY + 8 * (LPP - 1) : 0;
     static_assert(LPP == 1 || LPP == 2 || LPP == 4, "1, 2 or 4 lanes per particle");
     static_assert(F >= 1, "at least one field per lane");
 };
@@ -938,7 +939,10 @@ __device__ void p2g_item(const P2GArgs& A, int64_t t, int64_t a, int64_t b, floa
         // the run (record, splines, bin, affine form) and writes it to the
         // table; in sub-step q the run's lanes read entry (q, run).  Entries
         // are sub-step-major so that the 8 runs' entries of one sub-step fall
-        // on different banks.  The ring holds one group (DEPTH == LPP): the
+        // on different banks, and the entries of sub-step q are shifted by 8 q
+        // floats so that the 8 lanes of a quarter warp (2 runs x 4 sub-steps)
+        // write to different banks too (ENTRY * 8 is a multiple of 32).  The
+        // ring holds one group (DEPTH == LPP): the
         // next group's records are issued once the entries are written and
         // arrive during the sub-steps.  Same arithmetic as the loop below.
         static_assert(C::DEPTH == LPP, "one group in the ring");
@@ -970,7 +974,8 @@ __device__ void p2g_item(const P2GArgs& A, int64_t t, int64_t a, int64_t b, floa
                 }
                 float E[C::F], G[C::F][3];
                 centre_form(cp, sp, E, G);
-                float4* e = reinterpret_cast<float4*>(table + (h * C::RUNS + run) * C::ENTRY);
+                float4* e =
+                    reinterpret_cast<float4*>(table + (h * C::RUNS + run) * C::ENTRY + 8 * h);
                 e[0] = make_float4(sp[0].w[0], sp[0].w[1], sp[0].w[2], sp[0].w[3]);
                 e[1] = make_float4(sp[1].w[0], sp[1].w[1], sp[1].w[2], sp[1].w[3]);
                 e[2] = make_float4(sp[2].w[0], sp[2].w[1], sp[2].w[2], sp[2].w[3]);
@@ -986,7 +991,7 @@ __device__ void p2g_item(const P2GArgs& A, int64_t t, int64_t a, int64_t b, floa
 #pragma unroll
             for (int q = 0; q < LPP; ++q) issue(s0 + LPP + q);
             for (int q = 0; q < LPP; ++q) {
-                const float* ef = table + (q * C::RUNS + run) * C::ENTRY;
+                const float* ef = table + (q * C::RUNS + run) * C::ENTRY + 8 * q;
                 const float4* e = reinterpret_cast<const float4*>(ef);
                 const float wx = ef[h];
                 const float4 wy4 = e[1], wz4 = e[2], me = e[3], g0 = e[4], g1 = e[5], g2 = e[6];
